@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Benchmark of the batched ML-KEM NTT + iNTT engine (one JSON line on rank 0).
+
+Workload (the configuration the headline metric is quoted on): 262,144
+polynomials per GPU (N=256 int16 coefficients, seeded uniform in [0, q)),
+forward NTT and inverse NTT as separate batched launches.  A step is one
+forward launch plus one inverse launch over 262,144 polynomials each; the
+value is round trips per second (polys/s), summed over ranks (weak scaling:
+every rank owns its own 262,144-polynomial batches, there is no exchange).
+
+L2 hygiene: four resident batches (4 x 128 MiB) rotate, so every launch reads
+a batch last touched three launches earlier (384 MiB of traffic in between,
+above the 126 MB L2).
+
+--impl reference times the reference's own C ntt()/invntt()
+(ntt_bench/ref, compiled unmodified into oracle/_ref) on all host threads, a
+4096-polynomial sample of the same workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+Q = 3329
+METRIC = "NTT+iNTT polys/s & %HBM roofline (bit-exact), 1xB200; batched p50/p99 us"
+BYTES_PER_POLY = 1024          # one transform: 512 B read + 512 B write
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20000)
+    p.add_argument("--warmup", type=int, default=200)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--npoly", type=int, default=262144)
+    p.add_argument("--e2e-steps", type=int, default=30)
+    p.add_argument("--cpu-seconds", type=float, default=6.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def config(npoly, world):
+    return {
+        "workload": f"batched forward NTT + inverse NTT as separate launches, {npoly} "
+                    "polynomials per GPU (N=256 int16, uniform [0,q), q=3329)",
+        "npoly_per_gpu": npoly,
+        "global_batch": npoly * world,
+        "parallelism": f"replicas/range-sharded x{world} (no collective on the data path)",
+        "l2": "4 resident batches rotated per launch (512 MiB working set > 126 MB L2)",
+    }
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="tk_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.device), "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.4)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def load_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def load_traffic(kernel: str, npoly: int):
+    """DRAM bytes per launch from the committed ncu summary (per polynomial,
+    scaled to this launch)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            per_poly = json.load(f)[kernel]["dram_bytes_per_poly"]
+        return per_poly * npoly
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------- CPU sides ----
+def cpu_oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import py_oracle
+    o = py_oracle.Oracle()
+    if py_oracle.RefKyber.available():
+        r = py_oracle.RefKyber(3)
+        return o, r.fn("ntt"), r.fn("invntt"), "reference"
+    return o, o.fn("tko_ntt"), o.fn("tko_invntt"), "port"
+
+
+def sample_input(n, seed=20240816):
+    import numpy as np
+    return np.random.default_rng(seed).integers(0, Q, size=(n, 256), dtype=np.int16)
+
+
+def cpu_baseline(seconds: float):
+    o, f, i, kind = cpu_oracle()
+    threads = os.cpu_count() or 1
+    rate, done = o.time_roundtrip(f, i, sample_input(4096), threads, seconds)
+    return {"value": rate, "unit": "polys/s", "cores": threads, "kind": kind,
+            "sample": f"NTT+iNTT round trips over a 4096-polynomial sample per thread, "
+                      f"repeated for {seconds:.0f} s on {threads} threads ({done} polys)"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    o, f, i, kind = cpu_oracle()
+    threads = os.cpu_count() or 1
+    sample = sample_input(4096)
+    for _ in range(args.warmup):
+        o.split_roundtrip(f, i, sample, threads)
+    times = [o.split_roundtrip(f, i, sample, threads) for _ in range(args.steps)]
+    total = sum(times)
+    value = 4096 * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "polys/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
+        "config": config(args.npoly, world),
+        "cpu_baseline": {"value": value, "unit": "polys/s", "cores": threads, "kind": kind,
+                         "sample": "each step: NTT then iNTT on a 4096-polynomial sample "
+                                   f"of the workload, split over {threads} threads"},
+        "e2e": {"value": value, "unit": "polys/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "latency_us": {"p50": 1e6 * statistics.median(times),
+                       "p99": 1e6 * sorted(times)[min(len(times) - 1, int(0.99 * len(times)))]},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------- ours ---
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import tensorkyber_b200 as tk
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    tk.init(local)
+    n = args.npoly
+    gen = np.random.default_rng(1000 + rank)
+    batches = [torch.from_numpy(gen.integers(0, Q, size=(n, 256), dtype=np.int16)).cuda()
+               for _ in range(4)]
+    stream = torch.cuda.current_stream()
+
+    def step(k):
+        tk.ntt(batches[(2 * k) % 4], stream=stream)
+        tk.invntt(batches[(2 * k + 1) % 4], stream=stream)
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+
+    K = args.steps
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * K + 1)]
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for k in range(K):
+        tk.ntt(batches[(2 * k) % 4], stream=stream)
+        ev[2 * k + 1].record(stream)
+        tk.invntt(batches[(2 * k + 1) % 4], stream=stream)
+        ev[2 * k + 2].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    total_ms = ev[0].elapsed_time(ev[2 * K])
+    fwd_ms = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(K)]
+    inv_ms = [ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(K)]
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    status = tk.device_status(local)
+    if status:
+        raise RuntimeError(f"kernel status flags {status:#x}")
+
+    # end to end through the host-memory API: pinned host batch in, result out
+    e2e = None
+    if args.e2e_steps > 0:
+        host = torch.from_numpy(gen.integers(0, Q, size=(n, 256), dtype=np.int16)).pin_memory()
+        h = host.numpy()
+        tk.ntt_host(h)
+        tk.invntt_host(h)
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            tk.ntt_host(h)
+            tk.invntt_host(h)
+        e2e_s = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": world * n * args.e2e_steps / e2e_s, "unit": "polys/s",
+               "h2d_bytes_per_step": 2 * n * 512, "d2h_bytes_per_step": 2 * n * 512,
+               "steps": args.e2e_steps,
+               "how": "tk_ntt_host + tk_invntt_host on a pinned host batch, wall clock"}
+
+    if rank == 0:
+        fwd_avg = sum(fwd_ms) / K
+        inv_avg = sum(inv_ms) / K
+        dom, avg = ("ntt_fwd", fwd_avg) if fwd_avg >= inv_avg else ("ntt_inv", inv_avg)
+        peak, peak_kind = load_peak()
+        achieved = BYTES_PER_POLY * n / (avg * 1e-3) / 1e9
+        traffic = load_traffic(dom, n)
+        lat_rt = sorted(f + i for f, i in zip(fwd_ms, inv_ms))
+        line = {
+            "metric": METRIC,
+            "value": world * n * K / (total_ms * 1e-3),
+            "unit": "polys/s",
+            "n_gpus": world, "steps": K, "warmup": args.warmup,
+            "ms_per_step": total_ms / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int16", "data": "synthetic",
+            "config": config(n, world),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                         if peak_kind == "measured" else "fallback 6650 GB/s",
+                         "bytes_per_launch": BYTES_PER_POLY * n},
+            "kernels_ms": {"ntt_fwd_avg": fwd_avg, "ntt_inv_avg": inv_avg},
+            "kernel_variant": "TMA bulk staging + int8 mma.sync m16n8k32/m16n8k16 (s8 x u8 -> s32)",
+            "latency_us": {"batch_roundtrip_p50": 1e3 * lat_rt[len(lat_rt) // 2],
+                           "batch_roundtrip_p99": 1e3 * lat_rt[min(K - 1, int(0.99 * K))]},
+            "e2e": e2e,
+            "gpu_launches": 2 * K,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

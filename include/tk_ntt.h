@@ -1,0 +1,107 @@
+/*
+ * tk_ntt.h -- C ABI of the B200 batched ML-KEM NTT engine (libtk.so).
+ *
+ * Ring Z_3329[x]/(x^256+1), polynomials are int16_t[256], batches are npoly
+ * contiguous polynomials (512 bytes each).  Conventions are those of the
+ * pqcrystals reference that TensorKyber validates against:
+ *
+ *   forward  = ntt()    ntt_bench/ref/ntt.h:10-11, ntt_bench/ref/ntt.c:80-95
+ *              standard-order input, bit-reversed output (128 degree-1
+ *              residues mod X^2 - zeta as coefficient pairs), twiddles in
+ *              Montgomery form so the output is in the normal domain.
+ *   inverse  = invntt() ntt_bench/ref/ntt.h:13-14, ntt_bench/ref/ntt.c:106-126
+ *              bit-reversed input, standard-order output, multiplied by the
+ *              Montgomery factor 2^16 (invntt(ntt(x)) == 2^16 * x mod q).
+ *
+ * Every output coefficient is congruent mod q to the reference's output on the
+ * same input.  The representatives are fixed and deterministic:
+ *   forward output in [0, q), inverse output centred in [-(q-1)/2, (q-1)/2].
+ * Both lie inside the bounds the reference's own outputs satisfy, so callers
+ * that reduce afterwards (ML-KEM's poly_reduce) see identical residues.
+ * Accepted inputs: forward any int16; inverse x <= 32245 (covers every input
+ * on which the reference itself does not overflow int16: |x| <= 9471 for
+ * ntt(), |x| <= 16383 for invntt()).
+ *
+ * Errors are returned as tk_status codes; no entry point exits or prints.
+ * All entry points are thread-safe.  Device entry points are asynchronous on
+ * the given stream (NULL = legacy default stream) and never allocate.
+ */
+#ifndef TK_NTT_H
+#define TK_NTT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TK_ABI_VERSION 1
+
+/* Same type as cudaStream_t; declared here so the header needs no CUDA headers. */
+typedef struct CUstream_st *tk_stream_t;
+
+typedef enum tk_status {
+  TK_SUCCESS = 0,
+  TK_ERR_INVALID_VALUE = 1,      /* NULL pointer, partially overlapping buffers, bad option */
+  TK_ERR_MISALIGNED = 2,         /* polynomial buffer not 16-byte aligned */
+  TK_ERR_TOO_LARGE = 3,          /* npoly above TK_MAX_POLYS */
+  TK_ERR_NO_DEVICE = 4,          /* no CUDA device, or not an sm_100 (B200-class) GPU */
+  TK_ERR_CUDA = 5,               /* a CUDA runtime call failed; tk_last_error() has the text */
+  TK_ERR_NOT_DEVICE_MEMORY = 6,  /* device entry point given a pointer the GPU cannot address */
+  TK_ERR_KERNEL_TIMEOUT = 7      /* a kernel's bounded wait gave up (see tk_device_status) */
+} tk_status;
+
+#define TK_MAX_POLYS ((size_t)1 << 32)
+
+/* ---- device-memory batch transforms ------------------------------------
+ * Replace the per-polynomial ntt()/invntt() (ntt_bench/ref/ntt.h:10-14) with
+ * one call per batch, and the reference's in-place batch kernels
+ * k_ntt_*(int16_t* d, int npoly) / k_invntt_*(int16_t* d, int npoly)
+ * (ntt_bench/ntt_bench.cu:62, 98, 182, 231).  polys must be device (or
+ * managed) memory, 16-byte aligned.  npoly == 0 is a successful no-op. */
+int tk_ntt(int16_t *polys, size_t npoly, tk_stream_t stream);
+int tk_invntt(int16_t *polys, size_t npoly, tk_stream_t stream);
+
+/* Out-of-place forms: in and out are either identical or disjoint. */
+int tk_ntt_oop(const int16_t *in, int16_t *out, size_t npoly, tk_stream_t stream);
+int tk_invntt_oop(const int16_t *in, int16_t *out, size_t npoly, tk_stream_t stream);
+
+/* ---- host-memory batch transforms (synchronous) -------------------------
+ * Same contract as ntt()/invntt() applied to each polynomial of a host array
+ * (ntt_bench/ref/ntt.h:10-14).  Copies in chunks through the current device
+ * with copy/compute overlap; pinned host memory runs at full link speed. */
+int tk_ntt_host(int16_t *polys, size_t npoly);
+int tk_invntt_host(int16_t *polys, size_t npoly);
+
+/* ---- runtime --------------------------------------------------------------
+ * tk_init: per-device set-up (constant tables, occupancy).  Every entry point
+ * runs it on first use of a device; call it explicitly before capturing a
+ * CUDA graph, because the set-up makes synchronous copies.  Corresponds to
+ * the reference's cudaMemcpyToSymbol(d_zetas) + setup_tc_matrices()
+ * (ntt_bench/ntt_bench.cu:932-933, ntt_bench/ntt_kernels.cuh:842-925). */
+int tk_init(int device);
+
+/* Reads and clears the kernel-side error flags of a device (bit 0: forward,
+ * bit 1: inverse kernel gave up on a bounded wait).  Synchronous. */
+int tk_device_status(int device, unsigned *flags);
+
+const char *tk_status_string(int status);
+/* Detail of the last failure on the calling thread ("" if none). */
+const char *tk_last_error(void);
+int tk_abi_version(void);
+
+/* ---- constant tables (no GPU needed) -------------------------------------
+ * The host matrix builder's output, for inspection and tests.  which:
+ *   0: M1[16][16]   1: M2[16][16][16]   2: MA[16][16][16]   3: Minv[16][16]
+ *      (int16 residues in [0, q), see tensorkyber_b200/csrc/tk_tables.h)
+ *   4: forward fragment tables   5: inverse fragment tables
+ * Copies min(bytes, size) bytes to out and returns the table size in bytes,
+ * or -TK_ERR_INVALID_VALUE.  Counterpart of setup_tc_matrices
+ * (ntt_bench/ntt_kernels.cuh:842-925), which builds the same maps. */
+long long tk_get_table(int which, void *out, size_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TK_NTT_H */

@@ -1,0 +1,195 @@
+"""tensorkyber_b200 -- B200 batched ML-KEM NTT / iNTT engine.
+
+Python face of the C ABI in ``include/tk_ntt.h`` (``libtk.so``).  The compute
+path is the sm_100a CUDA library; there is no CPU implementation here, and the
+module raises when the library cannot be loaded.
+
+Conventions follow the pqcrystals reference ``ntt()`` / ``invntt()``
+(TensorKyber ``ntt_bench/ref/ntt.c:80-126``): forward output is bit-reversed
+and lands in [0, q); inverse output is multiplied by 2^16 and centred in
+[-(q-1)/2, (q-1)/2].  Every coefficient is congruent mod q to the reference's.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+Q = 3329
+N = 256
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtk.so")
+CSRC = os.path.join(_HERE, "csrc")
+
+STATUS = {
+    0: "TK_SUCCESS", 1: "TK_ERR_INVALID_VALUE", 2: "TK_ERR_MISALIGNED",
+    3: "TK_ERR_TOO_LARGE", 4: "TK_ERR_NO_DEVICE", 5: "TK_ERR_CUDA",
+    6: "TK_ERR_NOT_DEVICE_MEMORY", 7: "TK_ERR_KERNEL_TIMEOUT",
+}
+
+
+class TKError(RuntimeError):
+    def __init__(self, status: int, detail: str = ""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {detail}")
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile libtk.so in-tree (nvcc, sm_100a)."""
+    with _lock:
+        if force or not os.path.exists(LIB_PATH) or _stale():
+            subprocess.run(["make", "-s", "-C", CSRC], check=True)
+    return LIB_PATH
+
+
+def _stale() -> bool:
+    t = os.path.getmtime(LIB_PATH)
+    for f in os.listdir(CSRC):
+        if f.endswith((".cu", ".cuh", ".cpp", ".h")) and os.path.getmtime(os.path.join(CSRC, f)) > t:
+            return True
+    hdr = os.path.join(_HERE, "..", "include")
+    if os.path.isdir(hdr):
+        for f in os.listdir(hdr):
+            if os.path.getmtime(os.path.join(hdr, f)) > t:
+                return True
+    return False
+
+
+def lib() -> ctypes.CDLL:
+    """Load libtk.so (building it first if it is missing or stale)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH) or _stale():
+        build()
+    L = ctypes.CDLL(LIB_PATH)
+    p16 = ctypes.c_void_p
+    for name in ("tk_ntt", "tk_invntt"):
+        f = getattr(L, name)
+        f.argtypes = [p16, ctypes.c_size_t, ctypes.c_void_p]
+        f.restype = ctypes.c_int
+    for name in ("tk_ntt_oop", "tk_invntt_oop"):
+        f = getattr(L, name)
+        f.argtypes = [p16, p16, ctypes.c_size_t, ctypes.c_void_p]
+        f.restype = ctypes.c_int
+    for name in ("tk_ntt_host", "tk_invntt_host"):
+        f = getattr(L, name)
+        f.argtypes = [p16, ctypes.c_size_t]
+        f.restype = ctypes.c_int
+    L.tk_init.argtypes = [ctypes.c_int]
+    L.tk_init.restype = ctypes.c_int
+    L.tk_device_status.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_uint)]
+    L.tk_device_status.restype = ctypes.c_int
+    L.tk_status_string.argtypes = [ctypes.c_int]
+    L.tk_status_string.restype = ctypes.c_char_p
+    L.tk_last_error.argtypes = []
+    L.tk_last_error.restype = ctypes.c_char_p
+    L.tk_abi_version.restype = ctypes.c_int
+    L.tk_get_table.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]
+    L.tk_get_table.restype = ctypes.c_longlong
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise TKError(rc, lib().tk_last_error().decode(errors="replace"))
+
+
+# ---------------------------------------------------------------- tables ----
+_TABLE_SHAPES = {0: (16, 16), 1: (16, 16, 16), 2: (16, 16, 16), 3: (16, 16)}
+
+
+def get_table(which: int) -> np.ndarray:
+    """Host matrix builder output (no GPU needed): 0 M1, 1 M2, 2 MA, 3 Minv as
+    int16 residues; 4 / 5 the forward / inverse fragment tables as raw uint32."""
+    L = lib()
+    size = L.tk_get_table(which, None, 0)
+    if size < 0:
+        raise TKError(-size, f"table {which}")
+    buf = np.zeros(size, dtype=np.uint8)
+    L.tk_get_table(which, buf.ctypes.data, size)
+    if which in _TABLE_SHAPES:
+        return buf.view(np.int16).reshape(_TABLE_SHAPES[which])
+    return buf.view(np.uint32)
+
+
+# ----------------------------------------------------------- transforms -----
+def _stream_ptr(stream) -> int:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return int(getattr(stream, "cuda_stream", stream))
+
+
+def _check_tensor(t) -> int:
+    import torch
+    if not isinstance(t, torch.Tensor) or t.dtype != torch.int16 or not t.is_cuda:
+        raise TypeError("expected a CUDA int16 tensor")
+    if not t.is_contiguous() or t.numel() % N:
+        raise ValueError("expected a contiguous tensor of whole int16[256] polynomials")
+    return t.numel() // N
+
+
+def ntt(polys, out=None, stream=None):
+    """Batched forward NTT of a CUDA int16 tensor (..., 256).  In place when
+    out is None or out is polys; returns the output tensor."""
+    n = _check_tensor(polys)
+    if out is None or out is polys:
+        _check(lib().tk_ntt(polys.data_ptr(), n, _stream_ptr(stream)))
+        return polys
+    if _check_tensor(out) != n:
+        raise ValueError("out has a different number of polynomials")
+    _check(lib().tk_ntt_oop(polys.data_ptr(), out.data_ptr(), n, _stream_ptr(stream)))
+    return out
+
+
+def invntt(polys, out=None, stream=None):
+    """Batched inverse NTT (with the 2^16 factor) of a CUDA int16 tensor."""
+    n = _check_tensor(polys)
+    if out is None or out is polys:
+        _check(lib().tk_invntt(polys.data_ptr(), n, _stream_ptr(stream)))
+        return polys
+    if _check_tensor(out) != n:
+        raise ValueError("out has a different number of polynomials")
+    _check(lib().tk_invntt_oop(polys.data_ptr(), out.data_ptr(), n, _stream_ptr(stream)))
+    return out
+
+
+def _host_arr(a: np.ndarray) -> int:
+    if not isinstance(a, np.ndarray) or a.dtype != np.int16 or not a.flags["C_CONTIGUOUS"]:
+        raise TypeError("expected a C-contiguous numpy int16 array")
+    if a.size % N:
+        raise ValueError("expected whole int16[256] polynomials")
+    return a.size // N
+
+
+def ntt_host(a: np.ndarray) -> np.ndarray:
+    """Forward NTT of host polynomials in place (synchronous, through the GPU)."""
+    _check(lib().tk_ntt_host(a.ctypes.data, _host_arr(a)))
+    return a
+
+
+def invntt_host(a: np.ndarray) -> np.ndarray:
+    """Inverse NTT of host polynomials in place (synchronous, through the GPU)."""
+    _check(lib().tk_invntt_host(a.ctypes.data, _host_arr(a)))
+    return a
+
+
+def init(device: int = 0) -> None:
+    _check(lib().tk_init(device))
+
+
+def device_status(device: int = 0) -> int:
+    flags = ctypes.c_uint(0)
+    rc = lib().tk_device_status(device, ctypes.byref(flags))
+    if rc not in (0, 7):
+        _check(rc)
+    return int(flags.value)

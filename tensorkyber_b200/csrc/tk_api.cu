@@ -1,0 +1,308 @@
+// tk_api.cu -- the C ABI (include/tk_ntt.h): argument checks, per-device set-up,
+// dispatch to the sm_100a kernels, and the chunked host-memory path.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+
+#include "../../include/tk_ntt.h"
+#include "tk_internal.h"
+#include "tk_tables.h"
+
+namespace {
+
+using tk::DeviceInfo;
+
+constexpr int kMaxDevices = 64;
+
+struct DeviceState {
+  std::mutex mu;
+  bool ready = false;
+  DeviceInfo info;
+  // host-path staging (allocated on the first host call for this device)
+  std::mutex host_mu;
+  int16_t* stage[3] = {nullptr, nullptr, nullptr};
+  cudaStream_t streams[3] = {nullptr, nullptr, nullptr};
+  size_t stage_polys = 0;
+};
+
+DeviceState g_dev[kMaxDevices];
+thread_local char t_err[256] = "";
+
+void set_err(const char* what, cudaError_t e) {
+  snprintf(t_err, sizeof(t_err), "%s: %s", what, cudaGetErrorString(e));
+}
+void set_msg(const char* msg) { snprintf(t_err, sizeof(t_err), "%s", msg); }
+
+int current_device(int* dev) {
+  cudaError_t e = cudaGetDevice(dev);
+  if (e != cudaSuccess) {
+    set_err("cudaGetDevice", e);
+    return TK_ERR_NO_DEVICE;
+  }
+  if (*dev < 0 || *dev >= kMaxDevices) {
+    set_msg("device ordinal out of range");
+    return TK_ERR_NO_DEVICE;
+  }
+  return TK_SUCCESS;
+}
+
+// Set-up of the current device; idempotent and thread-safe.
+int ensure_ready(int dev, DeviceInfo** out) {
+  DeviceState& S = g_dev[dev];
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.ready) {
+    cudaDeviceProp p;
+    cudaError_t e = cudaGetDeviceProperties(&p, dev);
+    if (e != cudaSuccess) {
+      set_err("cudaGetDeviceProperties", e);
+      return TK_ERR_NO_DEVICE;
+    }
+    if (p.major != 10 || p.minor != 0) {
+      snprintf(t_err, sizeof(t_err), "device %d is sm_%d%d; this build targets sm_100a only", dev,
+               p.major, p.minor);
+      return TK_ERR_NO_DEVICE;
+    }
+    S.info.device = dev;
+    S.info.num_sms = p.multiProcessorCount;
+    S.info.cc_major = p.major;
+    S.info.cc_minor = p.minor;
+    S.info.total_mem = p.totalGlobalMem;
+    if (!tk::mma_init_device(&S.info)) {
+      set_err("kernel set-up", cudaGetLastError());
+      return TK_ERR_CUDA;
+    }
+    S.ready = true;
+  }
+  *out = &S.info;
+  return TK_SUCCESS;
+}
+
+int check_device_ptr(const void* p) {
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_err("cudaPointerGetAttributes", e);
+    return TK_ERR_NOT_DEVICE_MEMORY;
+  }
+  if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return TK_SUCCESS;
+  if (a.type == cudaMemoryTypeHost && a.devicePointer != nullptr && a.devicePointer == p)
+    return TK_SUCCESS;  // mapped pinned memory with identical addresses
+  set_msg("pointer is not device-accessible memory");
+  return TK_ERR_NOT_DEVICE_MEMORY;
+}
+
+int run_device(bool inverse, const int16_t* in, int16_t* out, size_t npoly, cudaStream_t st) {
+  t_err[0] = 0;
+  if (npoly == 0) return TK_SUCCESS;
+  if (!in || !out) {
+    set_msg("NULL polynomial pointer");
+    return TK_ERR_INVALID_VALUE;
+  }
+  if (npoly > TK_MAX_POLYS) {
+    set_msg("npoly above TK_MAX_POLYS");
+    return TK_ERR_TOO_LARGE;
+  }
+  if (((uintptr_t)in & 15u) || ((uintptr_t)out & 15u)) {
+    set_msg("polynomial buffers must be 16-byte aligned");
+    return TK_ERR_MISALIGNED;
+  }
+  const uintptr_t bytes = (uintptr_t)npoly * 512u;
+  if (in != out) {
+    const uintptr_t a = (uintptr_t)in, b = (uintptr_t)out;
+    if (a < b + bytes && b < a + bytes) {
+      set_msg("input and output overlap without being identical");
+      return TK_ERR_INVALID_VALUE;
+    }
+  }
+  int dev;
+  int rc = current_device(&dev);
+  if (rc) return rc;
+  DeviceInfo* info;
+  rc = ensure_ready(dev, &info);
+  if (rc) return rc;
+  rc = check_device_ptr(in);
+  if (rc) return rc;
+  if (in != out && (rc = check_device_ptr(out))) return rc;
+  cudaError_t e = tk::launch_mma(inverse, in, out, (long long)npoly, *info, st);
+  if (e != cudaSuccess) {
+    set_err("kernel launch", e);
+    return TK_ERR_CUDA;
+  }
+  return TK_SUCCESS;
+}
+
+// Host path: chunks of stage_polys polynomials rotate through three device
+// buffers and three streams, so the H2D copy of chunk c+1, the kernel of chunk
+// c and the D2H copy of chunk c-1 overlap.
+int run_host(bool inverse, int16_t* polys, size_t npoly) {
+  t_err[0] = 0;
+  if (npoly == 0) return TK_SUCCESS;
+  if (!polys) {
+    set_msg("NULL polynomial pointer");
+    return TK_ERR_INVALID_VALUE;
+  }
+  if (npoly > TK_MAX_POLYS) {
+    set_msg("npoly above TK_MAX_POLYS");
+    return TK_ERR_TOO_LARGE;
+  }
+  int dev;
+  int rc = current_device(&dev);
+  if (rc) return rc;
+  DeviceInfo* info;
+  rc = ensure_ready(dev, &info);
+  if (rc) return rc;
+  DeviceState& S = g_dev[dev];
+  std::lock_guard<std::mutex> lk(S.host_mu);
+  cudaError_t e;
+  if (!S.stage[0]) {
+    S.stage_polys = 1u << 15;  // 16 MiB per chunk
+    for (int i = 0; i < 3; i++) {
+      if ((e = cudaMalloc(&S.stage[i], S.stage_polys * 512u)) != cudaSuccess ||
+          (e = cudaStreamCreateWithFlags(&S.streams[i], cudaStreamNonBlocking)) != cudaSuccess) {
+        set_err("host-path staging set-up", e);
+        for (int j = 0; j < 3; j++) {
+          if (S.stage[j]) cudaFree(S.stage[j]);
+          if (S.streams[j]) cudaStreamDestroy(S.streams[j]);
+          S.stage[j] = nullptr;
+          S.streams[j] = nullptr;
+        }
+        return TK_ERR_CUDA;
+      }
+    }
+  }
+  size_t done = 0;
+  int c = 0;
+  e = cudaSuccess;
+  while (done < npoly && e == cudaSuccess) {
+    const size_t n = (npoly - done < S.stage_polys) ? npoly - done : S.stage_polys;
+    cudaStream_t st = S.streams[c % 3];
+    int16_t* buf = S.stage[c % 3];
+    e = cudaMemcpyAsync(buf, polys + done * 256, n * 512u, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = tk::launch_mma(inverse, buf, buf, (long long)n, *info, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(polys + done * 256, buf, n * 512u, cudaMemcpyDeviceToHost, st);
+    done += n;
+    c++;
+  }
+  for (int i = 0; i < 3; i++) {
+    cudaError_t e2 = cudaStreamSynchronize(S.streams[i]);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e != cudaSuccess) {
+    set_err("host-path transform", e);
+    return TK_ERR_CUDA;
+  }
+  return TK_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tk_ntt(int16_t* polys, size_t npoly, tk_stream_t stream) {
+  return run_device(false, polys, polys, npoly, (cudaStream_t)stream);
+}
+int tk_invntt(int16_t* polys, size_t npoly, tk_stream_t stream) {
+  return run_device(true, polys, polys, npoly, (cudaStream_t)stream);
+}
+int tk_ntt_oop(const int16_t* in, int16_t* out, size_t npoly, tk_stream_t stream) {
+  return run_device(false, in, out, npoly, (cudaStream_t)stream);
+}
+int tk_invntt_oop(const int16_t* in, int16_t* out, size_t npoly, tk_stream_t stream) {
+  return run_device(true, in, out, npoly, (cudaStream_t)stream);
+}
+int tk_ntt_host(int16_t* polys, size_t npoly) { return run_host(false, polys, npoly); }
+int tk_invntt_host(int16_t* polys, size_t npoly) { return run_host(true, polys, npoly); }
+
+int tk_init(int device) {
+  t_err[0] = 0;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    set_err("cudaGetDeviceCount", e);
+    return TK_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= n || device >= kMaxDevices) {
+    set_msg("device ordinal out of range");
+    return TK_ERR_INVALID_VALUE;
+  }
+  int prev;
+  if ((e = cudaGetDevice(&prev)) != cudaSuccess) {
+    set_err("cudaGetDevice", e);
+    return TK_ERR_NO_DEVICE;
+  }
+  if ((e = cudaSetDevice(device)) != cudaSuccess) {
+    set_err("cudaSetDevice", e);
+    return TK_ERR_NO_DEVICE;
+  }
+  DeviceInfo* info;
+  int rc = ensure_ready(device, &info);
+  cudaSetDevice(prev);
+  return rc;
+}
+
+int tk_device_status(int device, unsigned* flags) {
+  t_err[0] = 0;
+  if (!flags) return TK_ERR_INVALID_VALUE;
+  int rc = tk_init(device);
+  if (rc) return rc;
+  int prev;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = tk::read_and_clear_status(flags);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    set_err("tk_device_status", e);
+    return TK_ERR_CUDA;
+  }
+  return *flags ? TK_ERR_KERNEL_TIMEOUT : TK_SUCCESS;
+}
+
+const char* tk_status_string(int status) {
+  switch (status) {
+    case TK_SUCCESS: return "success";
+    case TK_ERR_INVALID_VALUE: return "invalid value";
+    case TK_ERR_MISALIGNED: return "misaligned polynomial buffer";
+    case TK_ERR_TOO_LARGE: return "batch too large";
+    case TK_ERR_NO_DEVICE: return "no usable sm_100 device";
+    case TK_ERR_CUDA: return "CUDA runtime error";
+    case TK_ERR_NOT_DEVICE_MEMORY: return "pointer is not device memory";
+    case TK_ERR_KERNEL_TIMEOUT: return "kernel bounded wait timed out";
+    default: return "unknown status";
+  }
+}
+
+const char* tk_last_error(void) { return t_err; }
+int tk_abi_version(void) { return TK_ABI_VERSION; }
+
+long long tk_get_table(int which, void* out, size_t bytes) {
+  static tk::Matrices M;
+  static tk::FwdFrags FF;
+  static tk::InvFrags IF;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    tk::build_matrices(&M);
+    tk::build_fwd_frags(M, &FF);
+    tk::build_inv_frags(M, &IF);
+  });
+  const void* src;
+  size_t size;
+  switch (which) {
+    case 0: src = M.m1; size = sizeof(M.m1); break;
+    case 1: src = M.m2; size = sizeof(M.m2); break;
+    case 2: src = M.ma; size = sizeof(M.ma); break;
+    case 3: src = M.minv; size = sizeof(M.minv); break;
+    case 4: src = &FF; size = sizeof(FF); break;
+    case 5: src = &IF; size = sizeof(IF); break;
+    default: return -TK_ERR_INVALID_VALUE;
+  }
+  if (out) memcpy(out, src, bytes < size ? bytes : size);
+  return (long long)size;
+}
+
+}  // extern "C"

@@ -1,0 +1,175 @@
+// tk_tables.cpp -- host matrix builder: derives the four stage matrices of the
+// ML-KEM NTT by probing a modular restatement of the butterfly layers with unit
+// vectors (the construction of ntt_bench/ntt_kernels.cuh:831-925), then packs
+// them into 7-bit INT8 limb fragments in mma.sync register order.
+#include "tk_tables.h"
+
+#include <string.h>
+
+namespace tk {
+namespace {
+
+int64_t modq(int64_t v) {
+  v %= kQ;
+  return v < 0 ? v + kQ : v;
+}
+
+unsigned brv7(unsigned x) {
+  unsigned r = 0;
+  for (int b = 0; b < 7; b++) r |= ((x >> b) & 1u) << (6 - b);
+  return r;
+}
+
+// Twiddle k of the reference table (ntt_bench/ref/ntt.c:39-56) is
+// 2^16 * 17^brv7(k) mod q; its Montgomery product fqmul(z, v) = z * 2^-16 * v,
+// so in plain modular arithmetic the butterfly constant is 17^brv7(k).
+struct Twiddles {
+  int64_t w[128];
+  Twiddles() {
+    for (unsigned k = 0; k < 128; k++) {
+      int64_t acc = 1;
+      for (unsigned e = 0; e < brv7(k); e++) acc = acc * 17 % kQ;
+      w[k] = acc;
+    }
+  }
+};
+const Twiddles& tw() {
+  static const Twiddles t;
+  return t;
+}
+
+// Forward Cooley-Tukey layers with len in [len_lo, len_hi] (ref/ntt.c:80-95):
+// the twiddle index of (len, start) is 128/len + start/(2 len).
+void fwd_layers(int64_t r[256], unsigned len_hi, unsigned len_lo) {
+  for (unsigned len = len_hi; len >= len_lo; len >>= 1)
+    for (unsigned start = 0; start < 256; start += 2 * len) {
+      const int64_t z = tw().w[128 / len + start / (2 * len)];
+      for (unsigned j = start; j < start + len; j++) {
+        const int64_t t = z * r[j + len] % kQ;
+        const int64_t a = r[j];
+        r[j] = modq(a + t);
+        r[j + len] = modq(a - t);
+      }
+    }
+}
+
+// Inverse Gentleman-Sande layers with len in [len_lo, len_hi] (ref/ntt.c:106-122):
+// twiddle index 256/len - 1 - start/(2 len) (the k-- walk from 127).
+void inv_layers(int64_t r[256], unsigned len_lo, unsigned len_hi) {
+  for (unsigned len = len_lo; len <= len_hi; len <<= 1)
+    for (unsigned start = 0; start < 256; start += 2 * len) {
+      const int64_t z = tw().w[256 / len - 1 - start / (2 * len)];
+      for (unsigned j = start; j < start + len; j++) {
+        const int64_t a = r[j], b = r[j + len];
+        r[j] = modq(a + b);
+        r[j + len] = modq(z * modq(b - a));
+      }
+    }
+}
+
+// The final fqmul(r, 1441) of ref/ntt.c:124-125 multiplies by
+// 1441 * 2^-16 = 2^16 / 128 = 512 (mod q).
+constexpr int64_t kInvScale = 512;
+
+uint8_t limb(int64_t v, int g) { return (uint8_t)(g ? (v >> 7) : (v & 127)); }
+
+int64_t byte_weighted(int64_t c, int byte) { return modq(byte ? c * 256 : c); }
+
+}  // namespace
+
+void build_matrices(Matrices* M) {
+  int64_t v[256];
+  for (int m = 0; m < 16; m++) {
+    memset(v, 0, sizeof(v));
+    v[16 * m] = 1;
+    fwd_layers(v, 128, 16);
+    for (int i = 0; i < 16; i++) M->m1[i][m] = (int16_t)v[16 * i];
+
+    memset(v, 0, sizeof(v));
+    v[16 * m] = 1;
+    inv_layers(v, 16, 128);
+    for (int i = 0; i < 16; i++) M->minv[i][m] = (int16_t)modq(v[16 * i] * kInvScale);
+  }
+  for (int b = 0; b < 16; b++)
+    for (int c = 0; c < 16; c++) {
+      memset(v, 0, sizeof(v));
+      v[16 * b + c] = 1;
+      fwd_layers(v, 8, 2);
+      for (int co = 0; co < 16; co++) M->m2[b][co][c] = (int16_t)v[16 * b + co];
+
+      memset(v, 0, sizeof(v));
+      v[16 * b + c] = 1;
+      inv_layers(v, 2, 8);
+      for (int co = 0; co < 16; co++) M->ma[b][co][c] = (int16_t)v[16 * b + co];
+    }
+}
+
+// m16n8k32 A fragment, 8-bit: reg j byte e holds A[row][col] with
+// row = lane/4 (+8 for j odd), col = 4*(lane%4) + e (+16 for j >= 2).
+template <class F>
+static void pack_a_k32(F value, uint32_t out[32][4]) {
+  for (int lane = 0; lane < 32; lane++)
+    for (int j = 0; j < 4; j++) {
+      uint32_t w = 0;
+      for (int e = 0; e < 4; e++) {
+        const int row = (lane >> 2) + ((j & 1) ? 8 : 0);
+        const int col = 4 * (lane & 3) + e + ((j & 2) ? 16 : 0);
+        w |= (uint32_t)value(row, col) << (8 * e);
+      }
+      out[lane][j] = w;
+    }
+}
+
+// m16n8k16 A fragment, 8-bit: reg j byte e holds A[lane/4 + 8j][4*(lane%4) + e].
+template <class F>
+static void pack_a_k16(F value, uint32_t out[32][2]) {
+  for (int lane = 0; lane < 32; lane++)
+    for (int j = 0; j < 2; j++) {
+      uint32_t w = 0;
+      for (int e = 0; e < 4; e++)
+        w |= (uint32_t)value((lane >> 2) + 8 * j, 4 * (lane & 3) + e) << (8 * e);
+      out[lane][j] = w;
+    }
+}
+
+void build_fwd_frags(const Matrices& M, FwdFrags* F) {
+  for (int g = 0; g < 2; g++)
+    pack_a_k32([&](int i, int k) { return limb(byte_weighted(M.m1[i][k >> 1], k & 1), g); },
+               F->s1[g]);
+  int32_t corr[16];
+  for (int i = 0; i < 16; i++) {
+    int64_t rs = 0;
+    for (int m = 0; m < 16; m++) rs += M.m1[i][m];
+    corr[i] = (int32_t)modq(-32768 * rs);
+  }
+  for (int lane = 0; lane < 32; lane++) {
+    F->c1[lane][0] = corr[lane >> 2];
+    F->c1[lane][1] = corr[(lane >> 2) + 8];
+  }
+  for (int b = 0; b < 16; b++)
+    for (int s = 0; s < 2; s++)
+      pack_a_k16(
+          [&](int r, int k) {
+            const int co = 2 * (r & 7) + s;
+            const int c = 2 * fwd_slot_e(k >> 1) + s;
+            return limb(byte_weighted(M.m2[b][co][c], k & 1), r >> 3);
+          },
+          F->s2[b][s]);
+}
+
+void build_inv_frags(const Matrices& M, InvFrags* F) {
+  for (int b = 0; b < 16; b++)
+    for (int s = 0; s < 2; s++)
+      pack_a_k16(
+          [&](int r, int k) {
+            const int co = 2 * (r & 7) + s;
+            const int c = 2 * (k >> 1) + s;
+            return limb(byte_weighted(M.ma[b][co][c], k & 1), r >> 3);
+          },
+          F->sa[b][s]);
+  for (int g = 0; g < 2; g++)
+    pack_a_k32([&](int i, int k) { return limb(byte_weighted(M.minv[i][k >> 1], k & 1), g); },
+               F->sb[g]);
+}
+
+}  // namespace tk

@@ -1,0 +1,92 @@
+// tk_tables.h -- constant tables of the matrix-form NTT and their layout contract.
+//
+// The ring is Z_3329[x]/(x^256+1).  A polynomial r[256] is viewed as a 16x16 grid
+// r[16*m + c]: m is the "block" index (bits 4..7 of the coefficient index) and c
+// the position inside a 16-coefficient block (bits 0..3).  TensorKyber's method
+// (ntt_bench/ntt_kernels.cuh:140-148, 842-925) splits the 7-layer transform
+// into two constant linear maps mod q:
+//
+//   forward   stage 1: layers 1-4 (len 128..16) act on m only:
+//                      y[i][c]  = sum_m M1[i][m]      * x[m][c]
+//             stage 2: layers 5-7 (len 8..2) act inside block i:
+//                      z[i][c'] = sum_c M2[i][c'][c]  * y[i][c]
+//   inverse   stage A: GS layers len 2..8 inside block m:
+//                      y[m][c]  = sum_c' MA[m][c][c'] * x[m][c']
+//             stage B: GS layers len 16..128 and the final x1441 Montgomery
+//                      factor act on m:  z[i][c] = sum_m Minv[i][m] * y[m][c]
+//
+// The builder below derives all four by pushing unit vectors through a plain
+// modular restatement of the layer code, exactly the probing construction of
+// the reference's setup_tc_matrices (ntt_kernels.cuh:831-925).
+//
+// Device formulation (this build's own, see tk_ntt_mma.cu):
+//   * Data enter the int8 tensor cores as raw BYTES (u8 operand).  A 16-bit
+//     value v = b0 + 256*b1 contributes b0 and b1 on two K positions whose
+//     constants are C and (256*C mod q), so no CUDA-core limb split of the
+//     data is ever done.  Signed inputs are biased to unsigned first
+//     (x ^ 0x8000 = x + 32768 with the row sum folded into the accumulator
+//     init, or + 10q which is 0 mod q).
+//   * Every constant is stored as two 7-bit INT8 limbs, lo in [0,127] and
+//     hi in [0,26], on two accumulator groups g = 0, 1; the partial sums are
+//     recombined as S = D_lo + 128 * D_hi with one IMAD.
+//   * Stage-2 / stage-A matrices never mix even and odd c (len 8, 4, 2
+//     butterflies keep the parity), so each is applied as two 8x8 halves.
+#pragma once
+#include <stdint.h>
+
+namespace tk {
+
+constexpr int kN = 256;
+constexpr int kQ = 3329;
+
+// floor(2^32 / q): lazy Barrett, S - umulhi(S, kBarLazy) * q in [0, q + 8) for
+// S < 2^25.
+constexpr uint32_t kBarLazy = 1290167u;
+// ceil(2^38 / q): exact reduction floor(S / q) = umulhi(S, kBarExact) >> 6 for
+// every 0 <= S < 2^26 (the error term S * e / 2^38 < 2^-12 < 1/q).
+constexpr uint32_t kBarExact = 82570715u;
+
+// Bias that makes a signed int16 an unsigned 16-bit value without changing it
+// mod q: (x ^ 0x8000) + 522 = x + 33290 = x + 10q, valid for x <= 32245.
+constexpr uint32_t kBias10qPacked = 0x020A020Au;
+
+// ---- fragment tables (per lane, in the register order of mma.sync) -------
+// Forward stage 1: A = 16x32 s8, rows i (output block), K k = 2*m + byte.
+// Two accumulator groups (lo / hi limbs) -> two A fragments of 4 regs.
+// c1: accumulator init of group 0 for rows (lane>>2) and (lane>>2)+8: the
+// (-32768 * rowsum) mod q correction of the x ^ 0x8000 bias.
+// Forward stage 2: per block b and parity s, A = 16x16 s8 (m16n8k16):
+// rows r<8 -> group 0, r>=8 -> group 1, output c' = 2*(r&7) + s; K k = 2*slot
+// + byte, slot j holds c = 2*e(j) + s with e(j) = (j>>1) + 4*(j&1).
+struct FwdFrags {
+  uint32_t s1[2][32][4];
+  int32_t c1[32][2];
+  uint32_t s2[16][2][32][2];
+};
+
+// Inverse stage A: per block m and parity s, A = 16x16 s8; rows as in forward
+// stage 2 (output c' = 2*(r&7) + s); K k = 2*j + byte, slot j holds input
+// c = 2*j + s (natural order).  Inputs are biased by +10q (no correction).
+// Inverse stage B: A = 16x32 s8, rows i, K k = 2*m + byte; no correction.  The
+// kernel adds (q-1)/2 in the group-0 accumulator init to centre the output.
+struct InvFrags {
+  uint32_t sa[16][2][32][2];
+  uint32_t sb[2][32][4];
+};
+
+// Logical matrices (canonical residues in [0, q)).
+struct Matrices {
+  int16_t m1[16][16];        // [i][m]
+  int16_t m2[16][16][16];    // [block][c'][c]
+  int16_t ma[16][16][16];    // [block][c][c']  (output c, input c')
+  int16_t minv[16][16];      // [i][m]
+};
+
+void build_matrices(Matrices* M);
+void build_fwd_frags(const Matrices& M, FwdFrags* F);
+void build_inv_frags(const Matrices& M, InvFrags* F);
+
+// Slot order inside a forward stage-2 parity half.
+inline int fwd_slot_e(int slot) { return (slot >> 1) + 4 * (slot & 1); }
+
+}  // namespace tk

@@ -1,0 +1,121 @@
+"""Bit-level CPU model of the sm_100a kernels' integer arithmetic.
+
+It rebuilds the logical int8 operand matrices from the per-lane fragment tables
+that the library uploads (using the mma.sync register layouts of the PTX ISA),
+feeds them the same unsigned data bytes the kernels feed the tensor cores, and
+applies the same recombination and Barrett steps.  Agreement with the oracle
+here pins the tables and the arithmetic on the CPU; the GPU parity tests then
+only have to confirm the kernels' data movement.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+Q = 3329
+BAR_LAZY = 1290167        # floor(2^32 / q)
+BAR_EXACT = 82570715      # ceil(2^38 / q)
+
+
+def unpack_k32(frag: np.ndarray) -> np.ndarray:
+    """frag[32 lanes][4 regs] uint32 -> A[16][32] int8 (m16n8k32 row-major A)."""
+    A = np.zeros((16, 32), dtype=np.int64)
+    for lane in range(32):
+        for j in range(4):
+            w = int(frag[lane][j])
+            for e in range(4):
+                row = lane // 4 + (8 if j & 1 else 0)
+                col = 4 * (lane % 4) + e + (16 if j & 2 else 0)
+                A[row, col] = np.int8(np.uint8((w >> (8 * e)) & 255))
+    return A
+
+
+def unpack_k16(frag: np.ndarray) -> np.ndarray:
+    """frag[32 lanes][2 regs] uint32 -> A[16][16] int8 (m16n8k16 row-major A)."""
+    A = np.zeros((16, 16), dtype=np.int64)
+    for lane in range(32):
+        for j in range(2):
+            w = int(frag[lane][j])
+            for e in range(4):
+                A[lane // 4 + 8 * j, 4 * (lane % 4) + e] = np.int8(np.uint8((w >> (8 * e)) & 255))
+    return A
+
+
+def fwd_slot_e(slot: int) -> int:
+    return (slot >> 1) + 4 * (slot & 1)
+
+
+class FwdModel:
+    def __init__(self, words: np.ndarray):
+        w = np.asarray(words, dtype=np.uint32)
+        s1 = w[:256].reshape(2, 32, 4)
+        c1 = w[256:320].view(np.int32).reshape(32, 2)
+        s2 = w[320:].reshape(16, 2, 32, 2)
+        self.A1 = [unpack_k32(s1[g]) for g in range(2)]
+        corr = np.zeros(16, dtype=np.int64)
+        for lane in range(32):
+            corr[lane // 4] = c1[lane][0]
+            corr[lane // 4 + 8] = c1[lane][1]
+        self.corr = corr
+        self.A2 = [[unpack_k16(s2[b][s]) for s in range(2)] for b in range(16)]
+
+    def __call__(self, x: np.ndarray) -> np.ndarray:
+        x = np.asarray(x, dtype=np.int16).reshape(-1, 256)
+        P = x.shape[0]
+        u = (x.view(np.uint16).astype(np.int64) ^ 0x8000).reshape(P, 16, 16)  # [p][m][c]
+        X = np.stack([u & 255, u >> 8], axis=2).reshape(P, 32, 16)         # [p][k=2m+b][c]
+        D0 = self.corr[None, :, None] + np.einsum("ik,pkc->pic", self.A1[0], X)
+        D1 = np.einsum("ik,pkc->pic", self.A1[1], X)
+        S = D0 + 128 * D1
+        assert S.min() >= 0 and S.max() < (1 << 25), (S.min(), S.max())
+        mid = S - ((S * BAR_LAZY) >> 32) * Q                                 # [p][i][c]
+        assert mid.min() >= 0 and mid.max() < Q + 8
+        out = np.zeros((P, 256), dtype=np.int64)
+        for b in range(16):
+            for s in range(2):
+                cols = [2 * fwd_slot_e(j) + s for j in range(8)]
+                v = mid[:, b, cols]                                          # [p][slot]
+                B = np.stack([v & 255, v >> 8], axis=2).reshape(P, 16)       # [p][k]
+                D = B @ self.A2[b][s].T                                       # [p][row]
+                S2 = D[:, :8] + 128 * D[:, 8:]
+                assert S2.min() >= 0 and S2.max() < (1 << 26)
+                r = S2 - ((S2 * BAR_EXACT) >> 38) * Q
+                for a in range(8):
+                    out[:, 16 * b + 2 * a + s] = r[:, a]
+        assert out.min() >= 0 and out.max() < Q
+        return out.astype(np.int16)
+
+
+class InvModel:
+    def __init__(self, words: np.ndarray):
+        w = np.asarray(words, dtype=np.uint32)
+        sa = w[:2048].reshape(16, 2, 32, 2)
+        sb = w[2048:].reshape(2, 32, 4)
+        self.AA = [[unpack_k16(sa[b][s]) for s in range(2)] for b in range(16)]
+        self.AB = [unpack_k32(sb[g]) for g in range(2)]
+
+    def __call__(self, x: np.ndarray) -> np.ndarray:
+        x = np.asarray(x, dtype=np.int16).reshape(-1, 256)
+        assert x.max() <= 32245
+        P = x.shape[0]
+        u = (x.view(np.uint16).astype(np.int64) ^ 0x8000) + 522             # x + 10q
+        assert u.max() < 65536
+        mid = np.zeros((P, 256), dtype=np.int64)
+        for b in range(16):
+            for s in range(2):
+                v = u[:, [16 * b + 2 * j + s for j in range(8)]]
+                B = np.stack([v & 255, v >> 8], axis=2).reshape(P, 16)
+                D = B @ self.AA[b][s].T
+                S = D[:, :8] + 128 * D[:, 8:]
+                assert S.min() >= 0 and S.max() < (1 << 25)
+                r = S - ((S * BAR_LAZY) >> 32) * Q
+                for a in range(8):
+                    mid[:, 16 * b + 2 * a + s] = r[:, a]
+        m = mid.reshape(P, 16, 16)
+        X = np.stack([m & 255, m >> 8], axis=2).reshape(P, 32, 16)
+        D0 = 1664 + np.einsum("ik,pkc->pic", self.AB[0], X)
+        D1 = np.einsum("ik,pkc->pic", self.AB[1], X)
+        S = D0 + 128 * D1
+        assert S.min() >= 0 and S.max() < (1 << 26)
+        r = S - ((S * BAR_EXACT) >> 38) * Q - 1664
+        assert r.min() >= -1664 and r.max() <= 1664
+        return r.reshape(P, 256).astype(np.int16)

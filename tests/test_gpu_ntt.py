@@ -1,0 +1,216 @@
+"""GPU parity of the batched NTT / iNTT against the oracle (every coefficient).
+
+Bar: for every coefficient of every polynomial, canon(gpu) == canon(oracle),
+with canon(v) = v mod q in [0, q); integer work, so no tolerance.  In addition
+the GPU's own representatives are pinned: forward in [0, q), inverse centred
+in [-(q-1)/2, (q-1)/2], byte-identical from run to run.
+"""
+import ctypes
+import threading
+
+import numpy as np
+import pytest
+
+from conftest import rng
+from py_oracle import Q, canon
+
+pytestmark = pytest.mark.gpu
+
+
+def to_dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.int16)).cuda()
+
+
+def gpu_fwd(tk, torch, x):
+    t = to_dev(torch, x)
+    tk.ntt(t)
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def gpu_inv(tk, torch, x):
+    t = to_dev(torch, x)
+    tk.invntt(t)
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def check_fwd(out, ref):
+    assert out.min() >= 0 and out.max() < Q
+    bad = np.argwhere(out != canon(ref))
+    assert bad.size == 0, f"{len(bad)} mismatches, first at {bad[:4].tolist()}"
+
+
+def check_inv(out, ref):
+    assert out.min() >= -(Q // 2) and out.max() <= Q // 2
+    bad = np.argwhere(canon(out) != canon(ref))
+    assert bad.size == 0, f"{len(bad)} mismatches, first at {bad[:4].tolist()}"
+
+
+SIZES = [1, 2, 7, 8, 9, 31, 33, 64, 100, 257, 1000, 4096, 4097, 65541]
+
+
+@pytest.mark.parametrize("n", SIZES)
+def test_uniform_sizes(tk, cuda, oracle, n):
+    x = rng(n).integers(0, Q, size=(n, 256)).astype(np.int16)
+    check_fwd(gpu_fwd(tk, cuda, x), oracle.ntt(x))
+    check_inv(gpu_inv(tk, cuda, x), oracle.invntt(x))
+
+
+def test_roundtrip_matches_reference_chain(tk, cuda, oracle):
+    """The reference harness runs iNTT on its own NTT output
+    (ntt_bench/ntt_bench.cu:618-621, 949-955); do the same on the GPU."""
+    x = rng(11).integers(0, Q, size=(3000, 256)).astype(np.int16)
+    t = to_dev(cuda, x)
+    tk.ntt(t)
+    tk.invntt(t)
+    cuda.cuda.synchronize()
+    out = t.cpu().numpy()
+    check_inv(out, oracle.invntt(oracle.ntt(x)))
+    assert (canon(out) == canon(x.astype(np.int64) * 65536)).all()
+
+
+def test_reference_seed_inputs(tk, cuda, oracle):
+    """Inputs of the reference benchmark itself: glibc srand(20240816),
+    rand() % q (ntt_bench/ntt_bench.cu:942-945)."""
+    libc = ctypes.CDLL("libc.so.6")
+    libc.srand(20240816)
+    n = 4096
+    x = np.array([libc.rand() % Q for _ in range(n * 256)], dtype=np.int16).reshape(n, 256)
+    check_fwd(gpu_fwd(tk, cuda, x), oracle.ntt(x))
+    check_inv(gpu_inv(tk, cuda, x), oracle.invntt(x))
+
+
+def test_small_signed_inputs(tk, cuda, oracle):
+    """ML-KEM calls ntt() on CBD secrets in [-3, 3]; the TC-PACK inputs of the
+    reference are ternary (ntt_bench/ntt_bench.cu:782-785)."""
+    r = rng(3)
+    for lo, hi in ((-1, 2), (-2, 3), (-3, 4)):
+        x = r.integers(lo, hi, size=(2048, 256)).astype(np.int16)
+        check_fwd(gpu_fwd(tk, cuda, x), oracle.ntt(x))
+        check_inv(gpu_inv(tk, cuda, x), oracle.invntt(x))
+
+
+def test_edge_inputs(tk, cuda, oracle):
+    rows = [np.zeros(256), np.full(256, Q - 1), np.full(256, -(Q - 1)),
+            np.full(256, 9471), np.full(256, -9471),
+            np.tile([9471, -9471], 128), np.arange(256) * 37 % Q - 1664]
+    rows += [np.eye(256)[j] for j in range(256)]          # unit vectors = matrix columns
+    x = np.array(rows, dtype=np.int16)
+    check_fwd(gpu_fwd(tk, cuda, x), oracle.ntt(x))
+    y = np.concatenate([x, np.full((1, 256), 16383), np.full((1, 256), -16384),
+                        np.tile([16383, -16384], (1, 128))]).astype(np.int16)
+    check_inv(gpu_inv(tk, cuda, y), oracle.invntt(y))
+
+
+def test_zero_maps_to_zero(tk, cuda):
+    x = np.zeros((17, 256), dtype=np.int16)
+    assert (gpu_fwd(tk, cuda, x) == 0).all()
+    assert (gpu_inv(tk, cuda, x) == 0).all()
+
+
+def test_full_int16_domain(tk, cuda, oracle):
+    """Forward accepts any int16, inverse any x <= 32245: outputs stay exact mod q
+    (the reference overflows there, so compare with its result on canon(x))."""
+    r = rng(7)
+    x = r.integers(-32768, 32768, size=(1024, 256)).astype(np.int16)
+    check_fwd(gpu_fwd(tk, cuda, x), oracle.ntt(canon(x)))
+    y = r.integers(-32768, 32246, size=(1024, 256)).astype(np.int16)
+    check_inv(gpu_inv(tk, cuda, y), oracle.invntt(canon(y)))
+
+
+def test_out_of_place_and_guards(tk, cuda, oracle):
+    """Out-of-place equals in-place, and nothing outside [0, npoly) is touched."""
+    n = 1003
+    x = rng(5).integers(-3000, 3000, size=(n, 256)).astype(np.int16)
+    guard = 8
+    buf = cuda.full(((n + 2 * guard) * 256,), 0x5A5A, dtype=cuda.int16, device="cuda")
+    out = cuda.full_like(buf, 0x3C3C)
+    buf[guard * 256:(guard + n) * 256] = to_dev(cuda, x).flatten()
+    src = buf[guard * 256:(guard + n) * 256]
+    dst = out[guard * 256:(guard + n) * 256]
+    tk.ntt(src, out=dst)
+    cuda.cuda.synchronize()
+    o = out.cpu().numpy()
+    assert (o[:guard * 256] == 0x3C3C).all() and (o[(guard + n) * 256:] == 0x3C3C).all()
+    check_fwd(o[guard * 256:(guard + n) * 256].reshape(n, 256), oracle.ntt(x))
+    b = buf.cpu().numpy()
+    assert (b[guard * 256:(guard + n) * 256].reshape(n, 256) == x).all(), "input modified"
+    tk.invntt(src)
+    cuda.cuda.synchronize()
+    b = buf.cpu().numpy()
+    assert (b[:guard * 256] == 0x5A5A).all() and (b[(guard + n) * 256:] == 0x5A5A).all()
+    check_inv(b[guard * 256:(guard + n) * 256].reshape(n, 256), oracle.invntt(x))
+
+
+def test_deterministic_bytes(tk, cuda):
+    x = rng(9).integers(-5000, 5000, size=(20000, 256)).astype(np.int16)
+    a = gpu_fwd(tk, cuda, x)
+    b = gpu_fwd(tk, cuda, x)
+    assert (a == b).all()
+    a = gpu_inv(tk, cuda, x)
+    b = gpu_inv(tk, cuda, x)
+    assert (a == b).all()
+
+
+def test_host_api_matches_device(tk, cuda, oracle):
+    n = (1 << 15) * 2 + 77   # spans several host-path chunks, ragged tail
+    x = rng(13).integers(0, Q, size=(n, 256)).astype(np.int16)
+    h = x.copy()
+    tk.ntt_host(h)
+    assert (h == gpu_fwd(tk, cuda, x)).all()
+    check_fwd(h[:5000], oracle.ntt(x[:5000]))
+    tk.invntt_host(h)
+    assert (canon(h) == canon(x.astype(np.int64) * 65536)).all()
+
+
+def test_non_default_stream_and_threads(tk, cuda, oracle):
+    xs = [rng(20 + i).integers(0, Q, size=(777 + 100 * i, 256)).astype(np.int16) for i in range(4)]
+    ts = [to_dev(cuda, x) for x in xs]
+    cuda.cuda.synchronize()
+    errs = []
+
+    def work(i):
+        try:
+            s = cuda.cuda.Stream()
+            with cuda.cuda.stream(s):
+                tk.ntt(ts[i], stream=s)
+            s.synchronize()
+        except Exception as e:  # pragma: no cover - reported below
+            errs.append(e)
+
+    th = [threading.Thread(target=work, args=(i,)) for i in range(4)]
+    [t.start() for t in th]
+    [t.join() for t in th]
+    assert not errs
+    for x, t in zip(xs, ts):
+        check_fwd(t.cpu().numpy(), oracle.ntt(x))
+
+
+def test_error_paths(tk, cuda):
+    L = tk.lib()
+    t = cuda.zeros(64 * 256 + 8, dtype=cuda.int16, device="cuda")
+    s = cuda.cuda.current_stream().cuda_stream
+    assert L.tk_ntt(t.data_ptr() + 2, 4, s) == 2          # misaligned
+    assert L.tk_ntt(t.data_ptr(), 0, s) == 0              # empty batch
+    assert L.tk_ntt(None, 4, s) == 1                      # NULL
+    host = np.zeros(4 * 256, dtype=np.int16)
+    assert L.tk_ntt(host.ctypes.data, 4, s) == 6          # host pointer to device API
+    assert L.tk_ntt_oop(t.data_ptr(), t.data_ptr() + 512, 4, s) == 1   # overlap
+    assert L.tk_ntt(t.data_ptr(), (1 << 32) + 1, s) == 3  # too large
+    assert tk.device_status(0) == 0
+
+
+def test_large_batch_every_coefficient(tk, cuda, oracle):
+    """2^20 polynomials (512 MiB), every coefficient against the oracle."""
+    n = 1 << 20
+    x = rng(21).integers(0, Q, size=(n, 256), dtype=np.int16)
+    t = to_dev(cuda, x)
+    tk.ntt(t)
+    cuda.cuda.synchronize()
+    check_fwd(t.cpu().numpy(), oracle.ntt(x))
+    tk.invntt(t)
+    cuda.cuda.synchronize()
+    out = t.cpu().numpy()
+    assert (canon(out) == canon(x.astype(np.int64) * 65536)).all()
+    assert tk.device_status(0) == 0
