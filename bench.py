@@ -46,6 +46,7 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=30)
     p.add_argument("--cpu-seconds", type=float, default=6.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--variant", type=int, default=-1, help="force a kernel variant (-1: auto)")
     return p.parse_args()
 
 
@@ -199,6 +200,9 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     tk.init(local)
+    if args.variant >= 0:
+        tk.set_variant(tk.FORWARD, args.variant)
+        tk.set_variant(tk.INVERSE, args.variant)
     n = args.npoly
     gen = np.random.default_rng(1000 + rank)
     batches = [torch.from_numpy(gen.integers(0, Q, size=(n, 256), dtype=np.int16)).cuda()
@@ -287,7 +291,8 @@ def run_ours(args):
                          if peak_kind == "measured" else "fallback 6650 GB/s",
                          "bytes_per_launch": BYTES_PER_POLY * n},
             "kernels_ms": {"ntt_fwd_avg": fwd_avg, "ntt_inv_avg": inv_avg},
-            "kernel_variant": "TMA bulk staging + int8 mma.sync m16n8k32/m16n8k16 (s8 x u8 -> s32)",
+            "kernel_variant": {"forward": tk.variant_name(tk.get_variant(tk.FORWARD, n)),
+                               "inverse": tk.variant_name(tk.get_variant(tk.INVERSE, n))},
             "latency_us": {"batch_roundtrip_p50": 1e3 * lat_rt[len(lat_rt) // 2],
                            "batch_roundtrip_p99": 1e3 * lat_rt[min(K - 1, int(0.99 * K))]},
             "e2e": e2e,

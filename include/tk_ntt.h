@@ -18,9 +18,9 @@
  *   forward output in [0, q), inverse output centred in [-(q-1)/2, (q-1)/2].
  * Both lie inside the bounds the reference's own outputs satisfy, so callers
  * that reduce afterwards (ML-KEM's poly_reduce) see identical residues.
- * Accepted inputs: forward any int16; inverse x <= 32245 (covers every input
- * on which the reference itself does not overflow int16: |x| <= 9471 for
- * ntt(), |x| <= 16383 for invntt()).
+ * Accepted inputs: any int16 (a superset of the inputs on which the
+ * reference itself does not overflow int16: |x| <= 9471 for ntt(),
+ * |x| <= 16383 for invntt()).
  *
  * Errors are returned as tk_status codes; no entry point exits or prints.
  * All entry points are thread-safe.  Device entry points are asynchronous on
@@ -85,6 +85,20 @@ int tk_init(int device);
 /* Reads and clears the kernel-side error flags of a device (bit 0: forward,
  * bit 1: inverse kernel gave up on a bounded wait).  Synchronous. */
 int tk_device_status(int device, unsigned *flags);
+
+/* ---- kernel variants ------------------------------------------------------
+ * The engine ships several kernel variants (CTA shape, pipeline depth) and
+ * picks one per direction and batch size.  tk_set_variant forces one for all
+ * later calls in the process (-1 restores automatic choice); tk_get_variant
+ * reports the choice for a batch size.  No reference counterpart: the
+ * reference binary times each of its variants from main()
+ * (ntt_bench/ntt_bench.cu:967-974). */
+#define TK_FORWARD 0
+#define TK_INVERSE 1
+int tk_variant_count(void);
+const char *tk_variant_name(int variant);
+int tk_set_variant(int direction, int variant);
+int tk_get_variant(int direction, size_t npoly);
 
 const char *tk_status_string(int status);
 /* Detail of the last failure on the calling thread ("" if none). */

@@ -94,6 +94,13 @@ def lib() -> ctypes.CDLL:
     L.tk_abi_version.restype = ctypes.c_int
     L.tk_get_table.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]
     L.tk_get_table.restype = ctypes.c_longlong
+    L.tk_variant_count.restype = ctypes.c_int
+    L.tk_variant_name.argtypes = [ctypes.c_int]
+    L.tk_variant_name.restype = ctypes.c_char_p
+    L.tk_set_variant.argtypes = [ctypes.c_int, ctypes.c_int]
+    L.tk_set_variant.restype = ctypes.c_int
+    L.tk_get_variant.argtypes = [ctypes.c_int, ctypes.c_size_t]
+    L.tk_get_variant.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -181,6 +188,26 @@ def invntt_host(a: np.ndarray) -> np.ndarray:
     """Inverse NTT of host polynomials in place (synchronous, through the GPU)."""
     _check(lib().tk_invntt_host(a.ctypes.data, _host_arr(a)))
     return a
+
+
+FORWARD, INVERSE = 0, 1
+
+
+def variant_count() -> int:
+    return lib().tk_variant_count()
+
+
+def variant_name(v: int) -> str:
+    return lib().tk_variant_name(v).decode()
+
+
+def set_variant(direction: int, variant: int) -> None:
+    """Force a kernel variant for a direction (-1: automatic choice)."""
+    _check(lib().tk_set_variant(direction, variant))
+
+
+def get_variant(direction: int, npoly: int) -> int:
+    return lib().tk_get_variant(direction, npoly)
 
 
 def init(device: int = 0) -> None:

@@ -5,6 +5,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "../../include/tk_ntt.h"
@@ -31,10 +32,32 @@ struct DeviceState {
 DeviceState g_dev[kMaxDevices];
 thread_local char t_err[256] = "";
 
+// Kernel variant choice: forced by tk_set_variant (>= 0) or picked by size.
+std::atomic<int> g_forced[2] = {{-1}, {-1}};
+
+const char* const kVariantNames[tk::kNumMmaVariants] = {
+    "mma.sync 4 warps x 32-poly tiles, 3-slot TMA ring",
+    "mma.sync 8 warps x 64-poly tiles, 3-slot TMA ring",
+    "mma.sync 4 warps x 32-poly tiles, 2-slot TMA ring",
+};
+
+int choose_variant(bool inverse, size_t npoly) {
+  const int f = g_forced[inverse ? 1 : 0].load(std::memory_order_relaxed);
+  if (f >= 0) return f;
+  (void)npoly;
+  return 0;
+}
+
 void set_err(const char* what, cudaError_t e) {
   snprintf(t_err, sizeof(t_err), "%s: %s", what, cudaGetErrorString(e));
 }
 void set_msg(const char* msg) { snprintf(t_err, sizeof(t_err), "%s", msg); }
+
+// Current device of the calling thread.  The first call on a thread also
+// binds the device's primary context to the thread (cudaSetDevice), because
+// the tensor-map encoder is a driver call that needs a current context even
+// when the thread has made no runtime call yet.
+thread_local int t_bound_device = -1;
 
 int current_device(int* dev) {
   cudaError_t e = cudaGetDevice(dev);
@@ -46,7 +69,22 @@ int current_device(int* dev) {
     set_msg("device ordinal out of range");
     return TK_ERR_NO_DEVICE;
   }
+  if (t_bound_device != *dev) {
+    if ((e = cudaSetDevice(*dev)) != cudaSuccess) {
+      set_err("cudaSetDevice", e);
+      return TK_ERR_NO_DEVICE;
+    }
+    t_bound_device = *dev;
+  }
   return TK_SUCCESS;
+}
+
+void set_launch_err(cudaError_t e) {
+  if (e == cudaErrorInvalidResourceHandle)
+    snprintf(t_err, sizeof(t_err), "cuTensorMapEncodeTiled failed (CUresult %d)",
+             tk::last_encode_result());
+  else
+    set_err("kernel launch", e);
 }
 
 // Set-up of the current device; idempotent and thread-safe.
@@ -127,9 +165,10 @@ int run_device(bool inverse, const int16_t* in, int16_t* out, size_t npoly, cuda
   rc = check_device_ptr(in);
   if (rc) return rc;
   if (in != out && (rc = check_device_ptr(out))) return rc;
-  cudaError_t e = tk::launch_mma(inverse, in, out, (long long)npoly, *info, st);
+  cudaError_t e = tk::launch_mma(inverse, choose_variant(inverse, npoly), in, out,
+                                 (long long)npoly, *info, st);
   if (e != cudaSuccess) {
-    set_err("kernel launch", e);
+    set_launch_err(e);
     return TK_ERR_CUDA;
   }
   return TK_SUCCESS;
@@ -182,7 +221,8 @@ int run_host(bool inverse, int16_t* polys, size_t npoly) {
     cudaStream_t st = S.streams[c % 3];
     int16_t* buf = S.stage[c % 3];
     e = cudaMemcpyAsync(buf, polys + done * 256, n * 512u, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = tk::launch_mma(inverse, buf, buf, (long long)n, *info, st);
+    if (e == cudaSuccess)
+      e = tk::launch_mma(inverse, choose_variant(inverse, n), buf, buf, (long long)n, *info, st);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(polys + done * 256, buf, n * 512u, cudaMemcpyDeviceToHost, st);
     done += n;
@@ -278,6 +318,29 @@ const char* tk_status_string(int status) {
 }
 
 const char* tk_last_error(void) { return t_err; }
+
+int tk_variant_count(void) { return tk::kNumMmaVariants; }
+
+const char* tk_variant_name(int variant) {
+  if (variant < 0 || variant >= tk::kNumMmaVariants) return "";
+  return kVariantNames[variant];
+}
+
+int tk_set_variant(int direction, int variant) {
+  t_err[0] = 0;
+  if ((direction != TK_FORWARD && direction != TK_INVERSE) || variant < -1 ||
+      variant >= tk::kNumMmaVariants) {
+    set_msg("tk_set_variant: bad direction or variant");
+    return TK_ERR_INVALID_VALUE;
+  }
+  g_forced[direction == TK_INVERSE ? 1 : 0].store(variant);
+  return TK_SUCCESS;
+}
+
+int tk_get_variant(int direction, size_t npoly) {
+  if (direction != TK_FORWARD && direction != TK_INVERSE) return -TK_ERR_INVALID_VALUE;
+  return choose_variant(direction == TK_INVERSE, npoly);
+}
 int tk_abi_version(void) { return TK_ABI_VERSION; }
 
 long long tk_get_table(int which, void* out, size_t bytes) {

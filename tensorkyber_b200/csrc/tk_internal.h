@@ -6,11 +6,19 @@
 
 namespace tk {
 
+// mma.sync kernel variants (CTA shape / pipeline depth):
+//   0: 4 warps, 32-polynomial tiles, 3 slots   (4 CTAs/SM)
+//   1: 8 warps, 64-polynomial tiles, 3 slots   (2 CTAs/SM)
+//   2: 4 warps, 32-polynomial tiles, 2 slots   (6 CTAs/SM)
+constexpr int kNumMmaVariants = 3;
+// Largest batch one kernel launch covers (TMA coordinates are signed 32-bit).
+constexpr long long kMaxLaunchPolys = 1ll << 30;
+
 struct DeviceInfo {
   int device = -1;
   int num_sms = 0;
   int cc_major = 0, cc_minor = 0;
-  int mma_ctas_per_sm[2] = {1, 1};  // [forward, inverse]
+  int mma_ctas_per_sm[2][kNumMmaVariants] = {{1, 1, 1}, {1, 1, 1}};  // [inverse][variant]
   size_t total_mem = 0;
 };
 
@@ -19,8 +27,12 @@ struct DeviceInfo {
 bool mma_init_device(DeviceInfo* info);
 
 // Batched transform of npoly polynomials, src -> dst (src == dst for in place).
-cudaError_t launch_mma(bool inverse, const int16_t* src, int16_t* dst, long long npoly,
-                       const DeviceInfo& info, cudaStream_t stream);
+cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* dst,
+                       long long npoly, const DeviceInfo& info, cudaStream_t stream);
+
+// CUresult of the calling thread's last tensor-map encode (launch_mma reports
+// cudaErrorInvalidResourceHandle when an encode failed).
+int last_encode_result();
 
 // Kernel-side error flags (bounded waits that gave up), read and reset.
 cudaError_t read_and_clear_status(unsigned* flags);

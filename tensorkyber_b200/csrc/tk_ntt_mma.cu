@@ -1,28 +1,41 @@
-// tk_ntt_mma.cu -- batched ML-KEM NTT / iNTT on sm_100a: TMA bulk staging +
-// int8 mma.sync tiles, one independent pipeline per warp.
+// tk_ntt_mma.cu -- batched ML-KEM NTT / iNTT on sm_100a: tensor-TMA staging +
+// int8 mma.sync tiles, CTA-cooperative persistent tiles.
 //
-// Work unit: 8 consecutive polynomials (4 KiB).  Each warp owns kSlots smem
-// slots of 8 padded rows (528 B per polynomial, the 16 B pad makes every
-// access pattern below bank-conflict free or 2-way at most) and streams units
-// u = warp_id, warp_id + n_warps, ... through them:
+// A CTA of W warps owns a ring of S shared-memory slots; each slot holds a
+// tile of 8*W polynomials in padded 528-byte rows (the 16-byte pad makes the
+// block-wise accesses below bank-conflict free).  The pad comes from the TMA
+// box itself: the global batch is described as a [npoly][128] uint32 tensor
+// and every copy moves a box of 8 rows x 132 words, whose last 4 words per row
+// are out of bounds (zero-filled on load, skipped on store); polynomials past
+// npoly are out of bounds the same way, so ragged tails need no special code.
+// CTAs walk tiles blockIdx.x, blockIdx.x + gridDim.x, ...; per tile:
 //
-//   TMA  cp.async.bulk global->smem, 8 x 512 B, completion on an mbarrier
-//   fwd  stage 1 (M1, per polynomial): ldmatrix.trans -> 4 x m16n8k32 s8.u8
-//        -> S = D_lo + 128 D_hi -> lazy Barrett -> parity-split rows in place
-//        stage 2 (M2, per block pair, 8 polynomials): ldmatrix -> 4 x
-//        m16n8k16 -> exact Barrett to [0, q) -> natural order in place
-//   inv  stage A (MA, per block): 8 B loads + byte_perm -> 2 x m16n8k16
-//        -> lazy Barrett -> natural order in place
-//        stage B (Minv, per polynomial): like fwd stage 1, output centred
-//   TMA  cp.async.bulk smem->global, 8 x 512 B; the slot is refilled once
-//        the store has been read out (wait_group.read).
+//   load     lane 0 of warp w: mbarrier.arrive.expect_tx + one tensor TMA for
+//            polynomials 8w .. 8w+7 of the tile
+//   forward  stage 1 (M1, layers 1-4), by polynomial: warp w, polys 8w..8w+7:
+//              ldmatrix.trans -> 4 x mma m16n8k32 s8.u8 -> S = D_lo + 128 D_hi
+//              -> lazy Barrett -> parity-split rows, in place
+//            CTA barrier
+//            stage 2 (M2, layers 5-7), by block: warp w, blocks (16/W)w ..:
+//              ldmatrix -> 4 x mma m16n8k16 -> exact Barrett to [0, q)
+//              -> natural order, in place
+//            CTA barrier, then lane 0 of warp w stores polys 8w .. 8w+7
+//   inverse  stage A (MA) by block (as forward stage 2, lazy Barrett, natural
+//            order), CTA barrier, stage B (Minv) by polynomial (as forward
+//            stage 1, output centred), then each warp stores its own polys
+//   store    tensor TMA smem -> global; a slot is refilled (two tiles ahead)
+//            after its store was read out (wait_group.read)
 //
-// Reference counterparts: k_ntt_2tc_tc_cc / k_invntt_2tc_tc_cc and
-// k_ntt_tc_cc_cp / k_invntt_tc_cc_cp (ntt_bench/ntt_bench.cu:61-131,
-// 181-277) with ntt_core / intt_core (ntt_bench/ntt_kernels.cuh:393-489,
-// 548-625).
+// Reference counterparts: the in-place batch kernels k_ntt_2tc_tc_cc /
+// k_invntt_2tc_tc_cc / k_ntt_tc_cc_cp / k_invntt_tc_cc_cp
+// (ntt_bench/ntt_bench.cu:61-131, 181-277) over ntt_core / intt_core
+// (ntt_bench/ntt_kernels.cuh:393-489, 548-625).
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <stdint.h>
+
+#include <mutex>
 
 #include "tk_internal.h"
 #include "tk_ptx.cuh"
@@ -30,222 +43,251 @@
 
 namespace tk {
 
-constexpr int kRowBytes = 528;                  // 512 B polynomial + 16 B pad
-constexpr int kUnit = 8;                        // polynomials per warp unit
-constexpr int kSlotBytes = kUnit * kRowBytes;   // 4224
-constexpr int kSlots = 3;                       // pipeline depth per warp
-constexpr int kWarpSmem = kSlots * kSlotBytes + 64;  // + mbarriers
-constexpr int kWarpsPerCta = 4;
-constexpr int kCtaThreads = 32 * kWarpsPerCta;
-constexpr int kCtaSmem = kWarpsPerCta * kWarpSmem;
-constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s bound on every mbarrier wait
+constexpr int kRowBytes = 528;                    // 512 B polynomial + 16 B pad
+constexpr int kWarpBoxBytes = 8 * kRowBytes;      // one TMA box: 8 padded rows
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // every mbarrier wait gives up after 2 s
 
 __device__ FwdFrags g_fwd;
 __device__ InvFrags g_inv;
 __device__ unsigned int g_status;
 
-// ---------------------------------------------------------------- forward --
-struct FwdRegs {
-  uint32_t a1[2][4];
-  int32_t c1lo, c1hi;
-  uint32_t a2[16][2][2];
+template <int W, int S>
+struct Cfg {
+  static constexpr int kWarps = W;
+  static constexpr int kThreads = 32 * W;
+  static constexpr int kTile = 8 * W;                 // polynomials per tile
+  static constexpr int kSlotBytes = kTile * kRowBytes;
+  static constexpr int kSlots = S;
+  static constexpr int kSmem = S * kSlotBytes + 16 * S;  // slots + mbarriers
+  static constexpr int kBlocksPerWarp = 16 / W;       // block-wise stages
+  static constexpr int kPairsPerWarp = kBlocksPerWarp / 2;
+  // CTAs per SM the shared memory allows; also the register cap for ptxas
+  static constexpr int kMinBlocks = (227 * 1024) / (kSmem + 1024);
+  static_assert(W == 4 || W == 8, "4 or 8 warps per CTA");
 };
 
-__device__ __forceinline__ void load_fwd_regs(FwdRegs& R, int lane) {
-#pragma unroll
-  for (int g = 0; g < 2; g++)
-#pragma unroll
-    for (int j = 0; j < 4; j++) R.a1[g][j] = g_fwd.s1[g][lane][j];
-  R.c1lo = g_fwd.c1[lane][0];
-  R.c1hi = g_fwd.c1[lane][1];
-#pragma unroll
-  for (int b = 0; b < 16; b++)
-#pragma unroll
-    for (int s = 0; s < 2; s++)
-#pragma unroll
-      for (int j = 0; j < 2; j++) R.a2[b][s][j] = g_fwd.s2[b][s][lane][j];
+__device__ __forceinline__ void cta_sync_named() {
+  asm volatile("bar.sync 1;" ::: "memory");
 }
 
-// Stage 1 of one polynomial whose row starts at smem address rb.
-__device__ __forceinline__ void fwd_stage1(const FwdRegs& R, uint32_t rb, uint32_t ld_off,
-                                           uint8_t* row, uint32_t w_even, uint32_t w_odd) {
-  uint32_t b0, b1, b2, b3;
-  ldsm_x4_t(rb + ld_off, b0, b1, b2, b3);
-  // x ^ 0x8000 = x + 32768 as an unsigned 16-bit value; the 32768 * rowsum
-  // term is cancelled by the group-0 accumulator init (c1).
-  b0 ^= 0x80008000u;
-  b1 ^= 0x80008000u;
-  b2 ^= 0x80008000u;
-  b3 ^= 0x80008000u;
-  const int32_t cinit[4] = {R.c1lo, R.c1lo, R.c1hi, R.c1hi};
+// ------------------------------------------------ shared building blocks ----
+// Stage over m (forward stage 1 / inverse stage B) of one polynomial whose B
+// operands (ldmatrix.trans of the natural-order row) are b0..b3.
+template <bool kInverse>
+__device__ __forceinline__ void stage_m(const uint32_t (&a)[2][4], int32_t c_lo, int32_t c_hi,
+                                        uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3,
+                                        uint8_t* row, uint32_t w_even, uint32_t w_odd,
+                                        uint32_t w_nat) {
+  const int32_t cinit[4] = {c_lo, c_lo, c_hi, c_hi};
   const int32_t zero[4] = {0, 0, 0, 0};
   int32_t lo0[4], hi0[4], lo1[4], hi1[4];
-  mma_k32(lo0, R.a1[0], b0, b1, cinit);
-  mma_k32(hi0, R.a1[1], b0, b1, zero);
-  mma_k32(lo1, R.a1[0], b2, b3, cinit);
-  mma_k32(hi1, R.a1[1], b2, b3, zero);
+  mma_k32(lo0, a[0], b0, b1, cinit);
+  mma_k32(hi0, a[1], b0, b1, zero);
+  mma_k32(lo1, a[0], b2, b3, cinit);
+  mma_k32(hi1, a[1], b2, b3, zero);
   uint32_t y0[4], y1[4];
 #pragma unroll
   for (int e = 0; e < 4; e++) {
-    y0[e] = red_lazy((uint32_t)lo0[e] + ((uint32_t)hi0[e] << 7));
-    y1[e] = red_lazy((uint32_t)lo1[e] + ((uint32_t)hi1[e] << 7));
+    const uint32_t s0 = (uint32_t)lo0[e] + ((uint32_t)hi0[e] << 7);
+    const uint32_t s1 = (uint32_t)lo1[e] + ((uint32_t)hi1[e] << 7);
+    if (kInverse) {  // centred: accumulators carry +(q-1)/2
+      y0[e] = red_exact(s0) - 1664u;
+      y1[e] = red_exact(s1) - 1664u;
+    } else {
+      y0[e] = red_lazy(s0);
+      y1[e] = red_lazy(s1);
+    }
   }
-  // regs: [0] (row i, c=2q), [1] (row i, c=2q+1), [2] (row i+8, c=2q), [3] (row i+8, c=2q+1);
-  // n-tile 1 is c+8.  Parity-split slots: (c=2q | c=8+2q) and (c=2q+1 | c=9+2q).
-  *(uint32_t*)(row + w_even) = pack2(y0[0], y1[0]);
-  *(uint32_t*)(row + w_odd) = pack2(y0[1], y1[1]);
-  *(uint32_t*)(row + w_even + 256) = pack2(y0[2], y1[2]);
-  *(uint32_t*)(row + w_odd + 256) = pack2(y0[3], y1[3]);
+  // D regs: [0] (row i, c=2q), [1] (row i, c=2q+1), [2]/[3] row i+8; n-tile 1 is c+8.
+  if (kInverse) {  // natural order
+    *(uint32_t*)(row + w_nat) = pack2(y0[0], y0[1]);
+    *(uint32_t*)(row + w_nat + 16) = pack2(y1[0], y1[1]);
+    *(uint32_t*)(row + w_nat + 256) = pack2(y0[2], y0[3]);
+    *(uint32_t*)(row + w_nat + 256 + 16) = pack2(y1[2], y1[3]);
+  } else {  // parity-split slots (c=2q | c=8+2q), (c=2q+1 | c=9+2q)
+    *(uint32_t*)(row + w_even) = pack2(y0[0], y1[0]);
+    *(uint32_t*)(row + w_odd) = pack2(y0[1], y1[1]);
+    *(uint32_t*)(row + w_even + 256) = pack2(y0[2], y1[2]);
+    *(uint32_t*)(row + w_odd + 256) = pack2(y0[3], y1[3]);
+  }
 }
 
-template <int I>
-__device__ __forceinline__ void fwd_stage2_pair(const FwdRegs& R, uint32_t slot, uint8_t* slotp,
-                                                uint32_t ld_off_h0, uint32_t ld_off_h1,
-                                                uint32_t st_off) {
-  uint32_t r[4];
-  constexpr int hb = (I >> 2) & 1;
-  ldsm_x4(slot + 32 * I + (hb ? ld_off_h1 : ld_off_h0), r[0], r[1], r[2], r[3]);
-  const int32_t zero[4] = {0, 0, 0, 0};
+// Block-wise stage (forward stage 2 / inverse stage A) for blocks I, I+1 of 8
+// polynomials.  r[0..3]: B operands (even I, odd I, even I+1, odd I+1).
+// Output: natural order, polynomials 2q and 2q+1 of the n-tile.
+template <bool kInverse>
+__device__ __forceinline__ void stage_c(const uint32_t (&a)[2][2][2], const int32_t (&ca)[2][2],
+                                        const uint32_t (&r)[4], uint8_t* out) {
 #pragma unroll
   for (int h = 0; h < 2; h++) {
+    const int32_t ce[4] = {ca[h][0], ca[h][0], 0, 0};
+    const int32_t co[4] = {ca[h][1], ca[h][1], 0, 0};
     int32_t de[4], dodd[4];
-    mma_k16(de, R.a2[I + h][0], r[2 * h], zero);
-    mma_k16(dodd, R.a2[I + h][1], r[2 * h + 1], zero);
-    const uint32_t e0 = red_exact((uint32_t)de[0] + ((uint32_t)de[2] << 7));
-    const uint32_t e1 = red_exact((uint32_t)de[1] + ((uint32_t)de[3] << 7));
-    const uint32_t o0 = red_exact((uint32_t)dodd[0] + ((uint32_t)dodd[2] << 7));
-    const uint32_t o1 = red_exact((uint32_t)dodd[1] + ((uint32_t)dodd[3] << 7));
-    *(uint32_t*)(slotp + st_off + 32 * (I + h)) = pack2(e0, o0);
-    *(uint32_t*)(slotp + st_off + kRowBytes + 32 * (I + h)) = pack2(e1, o1);
+    mma_k16(de, a[h][0], r[2 * h], ce);
+    mma_k16(dodd, a[h][1], r[2 * h + 1], co);
+    const uint32_t se0 = (uint32_t)de[0] + ((uint32_t)de[2] << 7);
+    const uint32_t se1 = (uint32_t)de[1] + ((uint32_t)de[3] << 7);
+    const uint32_t so0 = (uint32_t)dodd[0] + ((uint32_t)dodd[2] << 7);
+    const uint32_t so1 = (uint32_t)dodd[1] + ((uint32_t)dodd[3] << 7);
+    uint32_t e0, e1, o0, o1;
+    if (kInverse) {
+      e0 = red_lazy(se0); e1 = red_lazy(se1); o0 = red_lazy(so0); o1 = red_lazy(so1);
+    } else {
+      e0 = red_exact(se0); e1 = red_exact(se1); o0 = red_exact(so0); o1 = red_exact(so1);
+    }
+    *(uint32_t*)(out + 32 * h) = pack2(e0, o0);
+    *(uint32_t*)(out + kRowBytes + 32 * h) = pack2(e1, o1);
   }
 }
 
-// ---------------------------------------------------------------- inverse --
-struct InvRegs {
-  uint32_t aa[16][2][2];
-  uint32_t ab[2][4];
-};
-
-__device__ __forceinline__ void load_inv_regs(InvRegs& R, int lane) {
+// Block-wise stage of one tile for this warp: P block pairs x W n-tiles of 8
+// polynomials, the next unit's ldmatrix issued ahead of the current stores.
+// Inverse input is biased (x ^ 0x8000) and parity-split here; forward input
+// is already parity-split by stage 1.
+template <bool kInverse, int W, int P>
+__device__ __forceinline__ void block_stage(uint32_t slot, uint8_t* slotp, int blk0,
+                                            uint32_t ldc_off, uint32_t stc_off,
+                                            const uint32_t (&ac)[P][2][2][2],
+                                            const int32_t (&cc)[P][2][2]) {
+  constexpr int kIters = P * W;
+  uint32_t r[4];
+  ldsm_x4(slot + 32u * blk0 + ldc_off, r[0], r[1], r[2], r[3]);
 #pragma unroll
-  for (int b = 0; b < 16; b++)
+  for (int it = 0; it < kIters; it++) {
+    const int p = it / W, nt = it % W;
+    uint32_t n[4] = {0, 0, 0, 0};
+    if (it + 1 < kIters) {
+      const int p1 = (it + 1) / W, nt1 = (it + 1) % W;
+      ldsm_x4(slot + nt1 * 8 * kRowBytes + 32u * (blk0 + 2 * p1) + ldc_off, n[0], n[1], n[2],
+              n[3]);
+    }
+    uint32_t x[4];
+    if (kInverse) {
+      // r = (I: c 2q,2q+1 | I: c 8+2q,9+2q | I+1: ...); bias, then parity split
+      // into slots (c=2q | c=8+2q) and (c=2q+1 | c=9+2q)
+      const uint32_t x0 = r[0] ^ 0x80008000u, x1 = r[1] ^ 0x80008000u;
+      const uint32_t x2 = r[2] ^ 0x80008000u, x3 = r[3] ^ 0x80008000u;
+      x[0] = __byte_perm(x0, x1, 0x5410);
+      x[1] = __byte_perm(x0, x1, 0x7632);
+      x[2] = __byte_perm(x2, x3, 0x5410);
+      x[3] = __byte_perm(x2, x3, 0x7632);
+    } else {
 #pragma unroll
-    for (int s = 0; s < 2; s++)
+      for (int j = 0; j < 4; j++) x[j] = r[j];
+    }
+    stage_c<kInverse>(ac[p], cc[p], x,
+                      slotp + nt * 8 * kRowBytes + 32 * (blk0 + 2 * p) + stc_off);
 #pragma unroll
-      for (int j = 0; j < 2; j++) R.aa[b][s][j] = g_inv.sa[b][s][lane][j];
-#pragma unroll
-  for (int g = 0; g < 2; g++)
-#pragma unroll
-    for (int j = 0; j < 4; j++) R.ab[g][j] = g_inv.sb[g][lane][j];
-}
-
-template <int B>
-__device__ __forceinline__ void inv_stageA_block(const InvRegs& R, uint8_t* slotp,
-                                                 uint32_t ld_off, uint32_t st_off) {
-  const uint2 v = *(const uint2*)(slotp + ld_off + 32 * B);
-  // +10q bias: (x ^ 0x8000) + 522 per 16-bit half, no carry for x <= 32245.
-  const uint32_t a = (v.x ^ 0x80008000u) + kBias10qPacked;
-  const uint32_t b = (v.y ^ 0x80008000u) + kBias10qPacked;
-  const uint32_t ev = __byte_perm(a, b, 0x5410);  // c = 4q, 4q+2
-  const uint32_t od = __byte_perm(a, b, 0x7632);  // c = 4q+1, 4q+3
-  const int32_t zero[4] = {0, 0, 0, 0};
-  int32_t de[4], dodd[4];
-  mma_k16(de, R.aa[B][0], ev, zero);
-  mma_k16(dodd, R.aa[B][1], od, zero);
-  const uint32_t e0 = red_lazy((uint32_t)de[0] + ((uint32_t)de[2] << 7));
-  const uint32_t e1 = red_lazy((uint32_t)de[1] + ((uint32_t)de[3] << 7));
-  const uint32_t o0 = red_lazy((uint32_t)dodd[0] + ((uint32_t)dodd[2] << 7));
-  const uint32_t o1 = red_lazy((uint32_t)dodd[1] + ((uint32_t)dodd[3] << 7));
-  *(uint32_t*)(slotp + st_off + 32 * B) = pack2(e0, o0);
-  *(uint32_t*)(slotp + st_off + kRowBytes + 32 * B) = pack2(e1, o1);
-}
-
-__device__ __forceinline__ void inv_stageB(const InvRegs& R, uint32_t rb, uint32_t ld_off,
-                                           uint8_t* row, uint32_t w_off) {
-  uint32_t b0, b1, b2, b3;
-  ldsm_x4_t(rb + ld_off, b0, b1, b2, b3);
-  // +(q-1)/2 in the accumulator init so that S - q*floor(S/q) - 1664 is the
-  // centred representative in [-(q-1)/2, (q-1)/2].
-  const int32_t cinit[4] = {1664, 1664, 1664, 1664};
-  const int32_t zero[4] = {0, 0, 0, 0};
-  int32_t lo0[4], hi0[4], lo1[4], hi1[4];
-  mma_k32(lo0, R.ab[0], b0, b1, cinit);
-  mma_k32(hi0, R.ab[1], b0, b1, zero);
-  mma_k32(lo1, R.ab[0], b2, b3, cinit);
-  mma_k32(hi1, R.ab[1], b2, b3, zero);
-  uint32_t y0[4], y1[4];
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    y0[e] = red_exact((uint32_t)lo0[e] + ((uint32_t)hi0[e] << 7)) - 1664u;
-    y1[e] = red_exact((uint32_t)lo1[e] + ((uint32_t)hi1[e] << 7)) - 1664u;
+    for (int j = 0; j < 4; j++) r[j] = n[j];
   }
-  *(uint32_t*)(row + w_off) = pack2(y0[0], y0[1]);
-  *(uint32_t*)(row + w_off + 16) = pack2(y1[0], y1[1]);
-  *(uint32_t*)(row + w_off + 256) = pack2(y0[2], y0[3]);
-  *(uint32_t*)(row + w_off + 256 + 16) = pack2(y1[2], y1[3]);
+}
+
+// Stage over m for this warp's 8 polynomials, the next ldmatrix issued ahead.
+template <bool kInverse>
+__device__ __forceinline__ void poly_stage(uint32_t mine, uint8_t* minep, uint32_t ldt_off,
+                                           const uint32_t (&am)[2][4], int32_t cm_lo,
+                                           int32_t cm_hi, uint32_t w_even, uint32_t w_odd,
+                                           uint32_t w_nat) {
+  uint32_t b[4];
+  ldsm_x4_t(mine + ldt_off, b[0], b[1], b[2], b[3]);
+#pragma unroll
+  for (int p = 0; p < 8; p++) {
+    uint32_t n[4] = {0, 0, 0, 0};
+    if (p < 7) ldsm_x4_t(mine + (p + 1) * kRowBytes + ldt_off, n[0], n[1], n[2], n[3]);
+    if (kInverse)
+      stage_m<true>(am, cm_lo, cm_hi, b[0], b[1], b[2], b[3], minep + p * kRowBytes, 0, 0,
+                    w_nat);
+    else  // x ^ 0x8000 bias; the 32768 * rowsum term is cancelled by cm_lo/cm_hi
+      stage_m<false>(am, cm_lo, cm_hi, b[0] ^ 0x80008000u, b[1] ^ 0x80008000u,
+                     b[2] ^ 0x80008000u, b[3] ^ 0x80008000u, minep + p * kRowBytes, w_even,
+                     w_odd, 0);
+#pragma unroll
+    for (int j = 0; j < 4; j++) b[j] = n[j];
+  }
 }
 
 // ------------------------------------------------------------ the kernel ---
-template <bool kInverse>
-__global__ void __launch_bounds__(kCtaThreads)
-    k_ntt_mma(const int16_t* __restrict__ src, int16_t* __restrict__ dst, long long npoly) {
+template <bool kInverse, int W, int S>
+__global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
+    k_ntt_mma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_out,
+              int npoly) {
+  using C = Cfg<W, S>;
   extern __shared__ __align__(128) uint8_t smem[];
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const long long nunits = (npoly + kUnit - 1) / kUnit;
-  const long long gw = (long long)blockIdx.x * kWarpsPerCta + warp;
-  const long long nw = (long long)gridDim.x * kWarpsPerCta;
-  if (gw >= nunits) return;
-  const long long nmine = (nunits - gw + nw - 1) / nw;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int ntiles = (npoly + C::kTile - 1) / C::kTile;
+  if ((int)blockIdx.x >= ntiles) return;  // CTA-uniform
+  const int nmine = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
 
-  uint8_t* wsm = smem + warp * kWarpSmem;
-  const uint32_t slot0 = smem_u32(wsm);
-  const uint32_t bar0 = slot0 + kSlots * kSlotBytes;
+  const uint32_t smem0 = smem_u32(smem);
+  const uint32_t bar0 = smem0 + C::kSlots * C::kSlotBytes;
 
-  FwdRegs F;
-  InvRegs V;
-  if (kInverse)
-    load_inv_regs(V, lane);
-  else
-    load_fwd_regs(F, lane);
-
-  if (lane == 0) {
+  // ---- constants of this warp's role -> registers -------------------------
+  uint32_t am[2][4];                       // stage over m (fwd M1 / inv Minv)
+  int32_t cm_lo, cm_hi;                    // its accumulator init
+  uint32_t ac[C::kPairsPerWarp][2][2][2];  // block-wise stage, per (pair, block, parity)
+  int32_t cc[C::kPairsPerWarp][2][2];      // its group-0 accumulator init
+  const int blk0 = C::kBlocksPerWarp * warp;
 #pragma unroll
-    for (int s = 0; s < kSlots; s++) mbar_init(bar0 + 8 * s, 1);
+  for (int g = 0; g < 2; g++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) am[g][j] = kInverse ? g_inv.sb[g][lane][j] : g_fwd.s1[g][lane][j];
+  cm_lo = kInverse ? 1664 : g_fwd.c1[lane][0];
+  cm_hi = kInverse ? 1664 : g_fwd.c1[lane][1];
+#pragma unroll
+  for (int p = 0; p < C::kPairsPerWarp; p++)
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        const int b = blk0 + 2 * p + h;
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+          ac[p][h][s][j] = kInverse ? g_inv.sa[b][s][lane][j] : g_fwd.s2[b][s][lane][j];
+        cc[p][h][s] = kInverse ? g_inv.ca[b][s][lane] : 0;
+      }
+
+  if (tid == 0) {
+#pragma unroll
+    for (int s = 0; s < C::kSlots; s++) mbar_init(bar0 + 8 * s, W);
     fence_mbar_init();
   }
-  __syncwarp();
+  __syncthreads();
 
   const int q4 = lane & 3, g8 = lane >> 2;
-  // ldmatrix.trans row addresses (stage 1 / stage B): matrix j = lane/8 covers
+  // ldmatrix.trans rows of the stage over m: matrix j = lane/8 covers
   // m = (lane&7) + 8*(j&1), coefficients 8*(j>>1) .. +7.
   const uint32_t ldt_off = 32u * ((lane & 7) + 8 * ((lane >> 3) & 1)) + 16u * (lane >> 4);
-  // fwd stage-1 stores: row i = lane/4 (and +8), parity halves swapped for
-  // blocks with bit 2 set.
-  const uint32_t hb = (lane >> 4) & 1;
-  const uint32_t w_even = 32u * g8 + 16u * hb + 4u * q4;
-  const uint32_t w_odd = 32u * g8 + 16u * (hb ^ 1) + 4u * q4;
-  // fwd stage-2 ldmatrix rows: polynomial lane&7, block I + lane/16, half
-  // (lane/8)&1 (xor the block's bit 2).
-  const uint32_t s2_h0 = kRowBytes * (lane & 7) + 32u * (lane >> 4) + 16u * ((lane >> 3) & 1);
-  const uint32_t s2_h1 = kRowBytes * (lane & 7) + 32u * (lane >> 4) + 16u * (((lane >> 3) & 1) ^ 1);
-  // outputs of the block-wise stages: polynomial 2*q4 (and +1), pair lane/4.
-  const uint32_t st2_off = kRowBytes * (2 * q4) + 4u * g8;
-  // inverse stage-A loads: polynomial lane/4, coefficients 4*q4 .. +3.
-  const uint32_t la_off = kRowBytes * g8 + 8u * q4;
-  // inverse stage-B stores: row i = lane/4, coefficient pair 2*q4.
-  const uint32_t wb_off = 32u * g8 + 4u * q4;
+  // forward stage-1 stores: block i = lane/4 (and +8); the parity halves are
+  // swapped in blocks with bit 2 set (bank spread).
+  const uint32_t hb1 = (lane >> 4) & 1;
+  const uint32_t w_even = 32u * g8 + 16u * hb1 + 4u * q4;
+  const uint32_t w_odd = 32u * g8 + 16u * (hb1 ^ 1) + 4u * q4;
+  const uint32_t w_nat = 32u * g8 + 4u * q4;  // inverse stage-B stores
+  // block-wise stage: ldmatrix row = polynomial lane&7 of the n-tile, block
+  // (pair base) + lane/16; forward reads the parity halves (lane/8)&1 xor the
+  // block's bit 2 (uniform within a pair), inverse reads coefficient halves.
+  const uint32_t hbw = (uint32_t)((blk0 >> 2) & 1);
+  const uint32_t ldc_off = kRowBytes * (lane & 7) + 32u * (lane >> 4) +
+                           16u * (kInverse ? ((lane >> 3) & 1) : (((lane >> 3) & 1) ^ hbw));
+  const uint32_t stc_off = kRowBytes * (2 * q4) + 4u * g8;  // output pair lane/4, polys 2q, 2q+1
 
-  auto issue_load = [&](long long k, int slot_i) {
-    const long long u = gw + k * nw;
-    const long long left = npoly - u * kUnit;
-    const int valid = left < kUnit ? (int)left : kUnit;
+  // ---- TMA issue: lane 0 of each warp moves its 8 polynomials (one box) ----
+  auto issue_load = [&](int k, int slot_i) {
+    if (lane != 0) return;
+    const int tile = (int)blockIdx.x + k * (int)gridDim.x;
     const uint32_t bar = bar0 + 8 * slot_i;
-    if (lane == 0) mbar_expect_tx(bar, 512u * valid);
-    __syncwarp();
-    if (lane < valid)
-      bulk_g2s(slot0 + slot_i * kSlotBytes + lane * kRowBytes, src + (u * kUnit + lane) * kN,
-               512u, bar);
+    mbar_expect_tx(bar, kWarpBoxBytes);
+    tma_load_2d(smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes, &tm_in, 0,
+                tile * C::kTile + 8 * warp, bar);
+  };
+  auto issue_store = [&](int k, int slot_i) {
+    if (lane != 0) return;
+    const int tile = (int)blockIdx.x + k * (int)gridDim.x;
+    tma_store_2d(&tm_out, 0, tile * C::kTile + 8 * warp,
+                 smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes);
+    bulk_commit();
   };
 
   issue_load(0, 0);
@@ -253,126 +295,162 @@ __global__ void __launch_bounds__(kCtaThreads)
 
   int slot_i = 0;
   uint32_t phase = 0;
-  for (long long k = 0; k < nmine; k++) {
-    const uint32_t slot = slot0 + slot_i * kSlotBytes;
-    uint8_t* slotp = wsm + slot_i * kSlotBytes;
+  for (int k = 0; k < nmine; k++) {
+    const uint32_t slot = smem0 + slot_i * C::kSlotBytes;
+    uint8_t* slotp = smem + slot_i * C::kSlotBytes;
     const bool ok = mbar_wait_bounded(bar0 + 8 * slot_i, phase, kWaitLimitNs);
-    if (!__all_sync(0xffffffffu, ok)) {  // warp-uniform give-up
-      if (lane == 0) atomicOr(&g_status, kInverse ? 2u : 1u);
+    if (!__syncthreads_and(ok)) {  // CTA-uniform give-up
+      if (tid == 0) atomicOr(&g_status, kInverse ? 2u : 1u);
       break;
     }
+    // own polynomials of this warp: rows 8w .. 8w+7
+    const uint32_t mine = slot + 8 * warp * kRowBytes;
+    uint8_t* minep = slotp + 8 * warp * kRowBytes;
+
     if (!kInverse) {
-#pragma unroll 2
-      for (int p = 0; p < kUnit; p++)
-        fwd_stage1(F, slot + p * kRowBytes, ldt_off, slotp + p * kRowBytes, w_even, w_odd);
-      __syncwarp();
-      fwd_stage2_pair<0>(F, slot, slotp, s2_h0, s2_h1, st2_off);
-      fwd_stage2_pair<2>(F, slot, slotp, s2_h0, s2_h1, st2_off);
-      fwd_stage2_pair<4>(F, slot, slotp, s2_h0, s2_h1, st2_off);
-      fwd_stage2_pair<6>(F, slot, slotp, s2_h0, s2_h1, st2_off);
-      fwd_stage2_pair<8>(F, slot, slotp, s2_h0, s2_h1, st2_off);
-      fwd_stage2_pair<10>(F, slot, slotp, s2_h0, s2_h1, st2_off);
-      fwd_stage2_pair<12>(F, slot, slotp, s2_h0, s2_h1, st2_off);
-      fwd_stage2_pair<14>(F, slot, slotp, s2_h0, s2_h1, st2_off);
+      poly_stage<false>(mine, minep, ldt_off, am, cm_lo, cm_hi, w_even, w_odd, 0);
+      cta_sync_named();
+      block_stage<false, W>(slot, slotp, blk0, ldc_off, stc_off, ac, cc);
+      fence_proxy_async_smem();
+      cta_sync_named();
+      issue_store(k, slot_i);
     } else {
-      inv_stageA_block<0>(V, slotp, la_off, st2_off);
-      inv_stageA_block<1>(V, slotp, la_off, st2_off);
-      inv_stageA_block<2>(V, slotp, la_off, st2_off);
-      inv_stageA_block<3>(V, slotp, la_off, st2_off);
-      inv_stageA_block<4>(V, slotp, la_off, st2_off);
-      inv_stageA_block<5>(V, slotp, la_off, st2_off);
-      inv_stageA_block<6>(V, slotp, la_off, st2_off);
-      inv_stageA_block<7>(V, slotp, la_off, st2_off);
-      inv_stageA_block<8>(V, slotp, la_off, st2_off);
-      inv_stageA_block<9>(V, slotp, la_off, st2_off);
-      inv_stageA_block<10>(V, slotp, la_off, st2_off);
-      inv_stageA_block<11>(V, slotp, la_off, st2_off);
-      inv_stageA_block<12>(V, slotp, la_off, st2_off);
-      inv_stageA_block<13>(V, slotp, la_off, st2_off);
-      inv_stageA_block<14>(V, slotp, la_off, st2_off);
-      inv_stageA_block<15>(V, slotp, la_off, st2_off);
+      block_stage<true, W>(slot, slotp, blk0, ldc_off, stc_off, ac, cc);
+      cta_sync_named();
+      poly_stage<true>(mine, minep, ldt_off, am, cm_lo, cm_hi, 0, 0, w_nat);
+      fence_proxy_async_smem();
       __syncwarp();
-#pragma unroll 2
-      for (int p = 0; p < kUnit; p++)
-        inv_stageB(V, slot + p * kRowBytes, ldt_off, slotp + p * kRowBytes, wb_off);
-    }
-    // generic-proxy writes -> async-proxy bulk store
-    fence_proxy_async_smem();
-    __syncwarp();
-    {
-      const long long u = gw + k * nw;
-      const long long left = npoly - u * kUnit;
-      const int valid = left < kUnit ? (int)left : kUnit;
-      if (lane < valid) bulk_s2g(dst + (u * kUnit + lane) * kN, slot + lane * kRowBytes, 512u);
-      bulk_commit();
+      issue_store(k, slot_i);
     }
     if (k + 2 < nmine) {
-      // slot of unit k+2 last held unit k-1: its store must be read out.
-      bulk_wait_read<1>();
+      // the slot of tile k+2 last held tile k-1: its store must be read out
+      if (lane == 0) bulk_wait_read<1>();
       int s2 = slot_i + 2;
-      if (s2 >= kSlots) s2 -= kSlots;
+      if (s2 >= C::kSlots) s2 -= C::kSlots;
       issue_load(k + 2, s2);
     }
-    if (++slot_i == kSlots) {
+    if (++slot_i == C::kSlots) {
       slot_i = 0;
       phase ^= 1u;
     }
   }
-  bulk_wait_all();
+  if (lane == 0) bulk_wait_all();
 }
 
 // ------------------------------------------------------------ host side ----
+using Fn = void (*)(const CUtensorMap, const CUtensorMap, int);
+
+struct Variant {
+  Fn fn;
+  int threads;
+  int smem;
+  int tile;
+};
+
+template <bool I, int W, int S>
+constexpr Variant make_variant() {
+  return Variant{k_ntt_mma<I, W, S>, Cfg<W, S>::kThreads, Cfg<W, S>::kSmem, Cfg<W, S>::kTile};
+}
+
+// [inverse][variant]
+static const Variant kVariants[2][kNumMmaVariants] = {
+    {make_variant<false, 4, 3>(), make_variant<false, 8, 3>(), make_variant<false, 4, 2>()},
+    {make_variant<true, 4, 3>(), make_variant<true, 8, 3>(), make_variant<true, 4, 2>()},
+};
+
+static thread_local int g_last_encode_result = 0;
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  });
+  return fn;
+}
+
+// The batch as a [npoly][128] uint32 tensor; boxes of 8 polynomials x 132
+// words (the last 4 words are out of bounds: the smem row pad).
+static bool encode_batch_map(CUtensorMap* map, const int16_t* base, int npoly) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+  if (!enc) {
+    g_last_encode_result = -1;
+    return false;
+  }
+  const cuuint64_t dims[2] = {128, (cuuint64_t)npoly};
+  const cuuint64_t strides[1] = {512};
+  const cuuint32_t box[2] = {kRowBytes / 4, 8};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r =
+      enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, (void*)base, dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  g_last_encode_result = (int)r;
+  return r == CUDA_SUCCESS;
+}
+
+int last_encode_result() { return g_last_encode_result; }
+
 static bool upload_tables_current_device() {
   static Matrices M;
   static FwdFrags FF;
   static InvFrags IF;
-  static bool built = false;
-  if (!built) {
+  static std::once_flag once;
+  std::call_once(once, [] {
     build_matrices(&M);
     build_fwd_frags(M, &FF);
     build_inv_frags(M, &IF);
-    built = true;
-  }
+  });
   if (cudaMemcpyToSymbol(g_fwd, &FF, sizeof(FF)) != cudaSuccess) return false;
   if (cudaMemcpyToSymbol(g_inv, &IF, sizeof(IF)) != cudaSuccess) return false;
   const unsigned zero = 0;
-  if (cudaMemcpyToSymbol(g_status, &zero, sizeof(zero)) != cudaSuccess) return false;
-  if (cudaFuncSetAttribute(k_ntt_mma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           kCtaSmem) != cudaSuccess)
-    return false;
-  if (cudaFuncSetAttribute(k_ntt_mma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           kCtaSmem) != cudaSuccess)
-    return false;
-  return true;
+  return cudaMemcpyToSymbol(g_status, &zero, sizeof(zero)) == cudaSuccess;
 }
 
 bool mma_init_device(DeviceInfo* info) {
   if (!upload_tables_current_device()) return false;
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ntt_mma<false>, kCtaThreads,
-                                                    kCtaSmem) != cudaSuccess)
-    return false;
-  int per_sm_inv = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_inv, k_ntt_mma<true>, kCtaThreads,
-                                                    kCtaSmem) != cudaSuccess)
-    return false;
-  info->mma_ctas_per_sm[0] = per_sm > 0 ? per_sm : 1;
-  info->mma_ctas_per_sm[1] = per_sm_inv > 0 ? per_sm_inv : 1;
+  for (int inv = 0; inv < 2; inv++)
+    for (int v = 0; v < kNumMmaVariants; v++) {
+      const Variant& V = kVariants[inv][v];
+      if (cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, V.smem) !=
+          cudaSuccess)
+        return false;
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, V.fn, V.threads, V.smem) !=
+          cudaSuccess)
+        return false;
+      info->mma_ctas_per_sm[inv][v] = per_sm > 0 ? per_sm : 1;
+    }
   return true;
 }
 
-cudaError_t launch_mma(bool inverse, const int16_t* src, int16_t* dst, long long npoly,
-                       const DeviceInfo& info, cudaStream_t stream) {
-  const long long nunits = (npoly + kUnit - 1) / kUnit;
-  long long ctas = (nunits + kWarpsPerCta - 1) / kWarpsPerCta;
-  const long long cap = (long long)info.num_sms * info.mma_ctas_per_sm[inverse ? 1 : 0];
-  if (ctas > cap) ctas = cap;
-  if (ctas < 1) ctas = 1;
-  if (inverse)
-    k_ntt_mma<true><<<(unsigned)ctas, kCtaThreads, kCtaSmem, stream>>>(src, dst, npoly);
-  else
-    k_ntt_mma<false><<<(unsigned)ctas, kCtaThreads, kCtaSmem, stream>>>(src, dst, npoly);
-  return cudaGetLastError();
+cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* dst,
+                       long long npoly, const DeviceInfo& info, cudaStream_t stream) {
+  if (variant < 0 || variant >= kNumMmaVariants) variant = 0;
+  const Variant& V = kVariants[inverse ? 1 : 0][variant];
+  const long long cap = (long long)info.num_sms * info.mma_ctas_per_sm[inverse ? 1 : 0][variant];
+  // TMA coordinates are 32-bit: launch at most kMaxLaunchPolys per kernel.
+  for (long long done = 0; done < npoly; done += kMaxLaunchPolys) {
+    const int n = (int)((npoly - done) < kMaxLaunchPolys ? (npoly - done) : kMaxLaunchPolys);
+    CUtensorMap m_in, m_out;
+    if (!encode_batch_map(&m_in, src + done * 256, n)) return cudaErrorInvalidResourceHandle;
+    if (src == dst)
+      m_out = m_in;
+    else if (!encode_batch_map(&m_out, dst + done * 256, n))
+      return cudaErrorInvalidResourceHandle;
+    long long ctas = (n + V.tile - 1) / V.tile;
+    if (ctas > cap) ctas = cap;
+    if (ctas < 1) ctas = 1;
+    V.fn<<<(unsigned)ctas, V.threads, V.smem, stream>>>(m_in, m_out, n);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t read_and_clear_status(unsigned* flags) {

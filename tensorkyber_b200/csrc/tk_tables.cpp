@@ -159,14 +159,21 @@ void build_fwd_frags(const Matrices& M, FwdFrags* F) {
 
 void build_inv_frags(const Matrices& M, InvFrags* F) {
   for (int b = 0; b < 16; b++)
-    for (int s = 0; s < 2; s++)
+    for (int s = 0; s < 2; s++) {
       pack_a_k16(
           [&](int r, int k) {
             const int co = 2 * (r & 7) + s;
-            const int c = 2 * (k >> 1) + s;
+            const int c = 2 * fwd_slot_e(k >> 1) + s;
             return limb(byte_weighted(M.ma[b][co][c], k & 1), r >> 3);
           },
           F->sa[b][s]);
+      for (int lane = 0; lane < 32; lane++) {
+        const int co = 2 * (lane >> 2) + s;
+        int64_t rs = 0;
+        for (int c = 0; c < 16; c++) rs += M.ma[b][co][c];
+        F->ca[b][s][lane] = (int32_t)modq(-32768 * rs);
+      }
+    }
   for (int g = 0; g < 2; g++)
     pack_a_k32([&](int i, int k) { return limb(byte_weighted(M.minv[i][k >> 1], k & 1), g); },
                F->sb[g]);

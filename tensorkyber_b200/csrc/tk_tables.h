@@ -65,12 +65,15 @@ struct FwdFrags {
 };
 
 // Inverse stage A: per block m and parity s, A = 16x16 s8; rows as in forward
-// stage 2 (output c' = 2*(r&7) + s); K k = 2*j + byte, slot j holds input
-// c = 2*j + s (natural order).  Inputs are biased by +10q (no correction).
+// stage 2 (output c' = 2*(r&7) + s); K k = 2*slot + byte with the forward
+// stage-2 slot order (slot j holds input c = 2*e(j) + s).  Inputs are biased
+// with x ^ 0x8000; ca holds the group-0 accumulator init of row lane/4, the
+// (-32768 * rowsum) mod q correction.
 // Inverse stage B: A = 16x32 s8, rows i, K k = 2*m + byte; no correction.  The
 // kernel adds (q-1)/2 in the group-0 accumulator init to centre the output.
 struct InvFrags {
   uint32_t sa[16][2][32][2];
+  int32_t ca[16][2][32];
   uint32_t sb[2][32][4];
 };
 

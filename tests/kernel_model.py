@@ -89,23 +89,27 @@ class InvModel:
     def __init__(self, words: np.ndarray):
         w = np.asarray(words, dtype=np.uint32)
         sa = w[:2048].reshape(16, 2, 32, 2)
-        sb = w[2048:].reshape(2, 32, 4)
+        ca = w[2048:3072].view(np.int32).reshape(16, 2, 32)
+        sb = w[3072:].reshape(2, 32, 4)
         self.AA = [[unpack_k16(sa[b][s]) for s in range(2)] for b in range(16)]
+        self.corr = np.zeros((16, 2, 8), dtype=np.int64)          # [block][parity][row a]
+        for b in range(16):
+            for s in range(2):
+                for lane in range(32):
+                    self.corr[b, s, lane // 4] = ca[b][s][lane]
         self.AB = [unpack_k32(sb[g]) for g in range(2)]
 
     def __call__(self, x: np.ndarray) -> np.ndarray:
         x = np.asarray(x, dtype=np.int16).reshape(-1, 256)
-        assert x.max() <= 32245
         P = x.shape[0]
-        u = (x.view(np.uint16).astype(np.int64) ^ 0x8000) + 522             # x + 10q
-        assert u.max() < 65536
+        u = x.view(np.uint16).astype(np.int64) ^ 0x8000                   # x + 32768
         mid = np.zeros((P, 256), dtype=np.int64)
         for b in range(16):
             for s in range(2):
-                v = u[:, [16 * b + 2 * j + s for j in range(8)]]
+                v = u[:, [16 * b + 2 * fwd_slot_e(j) + s for j in range(8)]]
                 B = np.stack([v & 255, v >> 8], axis=2).reshape(P, 16)
                 D = B @ self.AA[b][s].T
-                S = D[:, :8] + 128 * D[:, 8:]
+                S = D[:, :8] + self.corr[b, s][None, :] + 128 * D[:, 8:]
                 assert S.min() >= 0 and S.max() < (1 << 25)
                 r = S - ((S * BAR_LAZY) >> 32) * Q
                 for a in range(8):
