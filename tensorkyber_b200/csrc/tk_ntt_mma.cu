@@ -8,7 +8,13 @@
 // and every copy moves a box of 8 rows x 132 words, whose last 4 words per row
 // are out of bounds (zero-filled on load, skipped on store); polynomials past
 // npoly are out of bounds the same way, so ragged tails need no special code.
-// CTAs walk tiles blockIdx.x, blockIdx.x + gridDim.x, ...; per tile:
+// CTA c owns the contiguous run of 8-polynomial units
+// [c*U/G, (c+1)*U/G) (U units, G CTAs), so CTAs differ by at most one unit of
+// work; it walks that run in tiles of W units (a warp whose unit lies past
+// the run issues no copy).  Launches use programmatic dependent launch: the
+// prologue (constants to registers, mbarrier set-up) overlaps the tail of the
+// previous kernel in the stream and griddepcontrol.wait precedes the first
+// global access.  Per tile:
 //
 //   load     lane 0 of warp w: mbarrier.arrive.expect_tx + one tensor TMA for
 //            polynomials 8w .. 8w+7 of the tile
@@ -23,8 +29,10 @@
 //   inverse  stage A (MA) by block (as forward stage 2, lazy Barrett, natural
 //            order), CTA barrier, stage B (Minv) by polynomial (as forward
 //            stage 1, output centred), then each warp stores its own polys
-//   store    tensor TMA smem -> global; a slot is refilled (two tiles ahead)
-//            after its store was read out (wait_group.read)
+//   store    tensor TMA smem -> global; at the top of the next iteration the
+//            slot is refilled (two tiles ahead) once that store was read out
+//            of smem (wait_group.read), so two loads stay in flight while a
+//            tile is computed
 //
 // Reference counterparts: the in-place batch kernels k_ntt_2tc_tc_cc /
 // k_invntt_2tc_tc_cc / k_ntt_tc_cc_cp / k_invntt_tc_cc_cp
@@ -216,9 +224,10 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  const int ntiles = (npoly + C::kTile - 1) / C::kTile;
-  if ((int)blockIdx.x >= ntiles) return;  // CTA-uniform
-  const int nmine = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int nunits = (npoly + 7) >> 3;
+  const int u_begin = (int)((long long)blockIdx.x * nunits / gridDim.x);
+  const int u_end = (int)((long long)(blockIdx.x + 1) * nunits / gridDim.x);
+  const int nmine = (u_end - u_begin + W - 1) / W;  // tiles of this CTA (CTA-uniform)
 
   const uint32_t smem0 = smem_u32(smem);
   const uint32_t bar0 = smem0 + C::kSlots * C::kSlotBytes;
@@ -254,6 +263,11 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
     fence_mbar_init();
   }
   __syncthreads();
+  // Everything above overlaps the previous kernel in the stream; from here on
+  // global memory that it may have written is read.
+  grid_dependency_wait();
+  grid_launch_dependents();
+  if (nmine == 0) return;  // CTA-uniform
 
   const int q4 = lane & 3, g8 = lane >> 2;
   // ldmatrix.trans rows of the stage over m: matrix j = lane/8 covers
@@ -276,17 +290,21 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
   // ---- TMA issue: lane 0 of each warp moves its 8 polynomials (one box) ----
   auto issue_load = [&](int k, int slot_i) {
     if (lane != 0) return;
-    const int tile = (int)blockIdx.x + k * (int)gridDim.x;
+    const int unit = u_begin + k * W + warp;
     const uint32_t bar = bar0 + 8 * slot_i;
-    mbar_expect_tx(bar, kWarpBoxBytes);
-    tma_load_2d(smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes, &tm_in, 0,
-                tile * C::kTile + 8 * warp, bar);
+    if (unit < u_end) {
+      mbar_expect_tx(bar, kWarpBoxBytes);
+      tma_load_2d(smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes, &tm_in, 0, 8 * unit,
+                  bar);
+    } else {
+      mbar_expect_tx(bar, 0);  // arrive only
+    }
   };
   auto issue_store = [&](int k, int slot_i) {
     if (lane != 0) return;
-    const int tile = (int)blockIdx.x + k * (int)gridDim.x;
-    tma_store_2d(&tm_out, 0, tile * C::kTile + 8 * warp,
-                 smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes);
+    const int unit = u_begin + k * W + warp;
+    if (unit < u_end)
+      tma_store_2d(&tm_out, 0, 8 * unit, smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes);
     bulk_commit();
   };
 
@@ -302,6 +320,15 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
     if (!__syncthreads_and(ok)) {  // CTA-uniform give-up
       if (tid == 0) atomicOr(&g_status, kInverse ? 2u : 1u);
       break;
+    }
+    if (k + 2 < nmine) {
+      // refill early: the slot of tile k+2 last held tile k-1, whose compute
+      // finished before the barrier above; its store (issued by this lane,
+      // for this warp's rows) must have been read out of smem.
+      if (lane == 0) bulk_wait_read<0>();
+      int s2 = slot_i + 2;
+      if (s2 >= C::kSlots) s2 -= C::kSlots;
+      issue_load(k + 2, s2);
     }
     // own polynomials of this warp: rows 8w .. 8w+7
     const uint32_t mine = slot + 8 * warp * kRowBytes;
@@ -321,13 +348,6 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
       fence_proxy_async_smem();
       __syncwarp();
       issue_store(k, slot_i);
-    }
-    if (k + 2 < nmine) {
-      // the slot of tile k+2 last held tile k-1: its store must be read out
-      if (lane == 0) bulk_wait_read<1>();
-      int s2 = slot_i + 2;
-      if (s2 >= C::kSlots) s2 -= C::kSlots;
-      issue_load(k + 2, s2);
     }
     if (++slot_i == C::kSlots) {
       slot_i = 0;
@@ -446,8 +466,17 @@ cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* d
     long long ctas = (n + V.tile - 1) / V.tile;
     if (ctas > cap) ctas = cap;
     if (ctas < 1) ctas = 1;
-    V.fn<<<(unsigned)ctas, V.threads, V.smem, stream>>>(m_in, m_out, n);
-    const cudaError_t e = cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ctas);
+    cfg.blockDim = dim3((unsigned)V.threads);
+    cfg.dynamicSmemBytes = (size_t)V.smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, V.fn, m_in, m_out, n);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
