@@ -52,7 +52,7 @@ def build(force: bool = False) -> str:
 def _stale() -> bool:
     t = os.path.getmtime(LIB_PATH)
     for f in os.listdir(CSRC):
-        if f.endswith((".cu", ".cuh", ".cpp", ".h")) and os.path.getmtime(os.path.join(CSRC, f)) > t:
+        if f.endswith((".cu", ".cuh", ".cpp", ".c", ".h")) and os.path.getmtime(os.path.join(CSRC, f)) > t:
             return True
     hdr = os.path.join(_HERE, "..", "include")
     if os.path.isdir(hdr):

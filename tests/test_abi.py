@@ -1,0 +1,90 @@
+"""The C-ABI library loads and exports every entry point include/*.h declares;
+argument validation and the table / variant queries work without a GPU (no
+compute call is made here)."""
+import ctypes
+import glob
+import os
+import re
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+# header -> shared library that must export everything it declares
+LIBS = {"tk_ntt.h": "libtk.so", "tk_pqcrystals.h": "libtk_pqcrystals.so"}
+
+
+def declared_functions(header=None):
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        if header and os.path.basename(h) != header:
+            continue
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[a-z_0-9 ]+[\s\*]+(\w+)\s*\(", src, flags=re.M):
+            if m.group(1) not in ("if", "while", "defined", "sizeof"):
+                names.add(m.group(1))
+    return names
+
+
+def test_every_header_has_a_library():
+    headers = {os.path.basename(h) for h in glob.glob(os.path.join(ROOT, "include", "*.h"))}
+    assert headers <= set(LIBS), headers - set(LIBS)
+
+
+def test_every_declared_symbol_is_exported(tk):
+    assert {"tk_ntt", "tk_invntt", "tk_ntt_host", "tk_invntt_host"} <= declared_functions("tk_ntt.h")
+    for header, so in LIBS.items():
+        names = declared_functions(header)
+        assert names, header
+        lib = ctypes.CDLL(os.path.join(ROOT, "tensorkyber_b200", so))
+        missing = [n for n in sorted(names) if not hasattr(lib, n)]
+        assert not missing, (header, missing)
+
+
+def test_abi_version_and_strings(tk):
+    L = tk.lib()
+    assert L.tk_abi_version() == 1
+    for code in range(8):
+        assert L.tk_status_string(code)
+    assert L.tk_status_string(99) == b"unknown status"
+    assert tk.variant_count() >= 1
+    assert all(tk.variant_name(v) for v in range(tk.variant_count()))
+    assert tk.variant_name(99) == ""
+
+
+def test_argument_errors_before_any_device_work(tk):
+    """These return before the library touches the GPU."""
+    L = tk.lib()
+    assert L.tk_ntt(None, 0, None) == 0                       # empty batch: no-op
+    assert L.tk_ntt(None, 5, None) == 1                       # NULL
+    assert L.tk_invntt_oop(None, None, 5, None) == 1
+    buf = np.zeros(8 * 256 + 16, dtype=np.int16)
+    base = (buf.ctypes.data + 15) & ~15
+    assert L.tk_ntt(base + 2, 4, None) == 2                   # misaligned
+    assert L.tk_ntt(base, (1 << 32) + 1, None) == 3           # too large
+    assert L.tk_ntt_oop(base, base + 512, 4, None) == 1       # partial overlap
+    assert L.tk_ntt_host(None, 3) == 1
+    assert L.tk_ntt_host(None, 0) == 0
+    assert b"aligned" in L.tk_last_error() or L.tk_last_error() == b""
+
+
+def test_variant_selection(tk):
+    L = tk.lib()
+    assert L.tk_set_variant(tk.FORWARD, 99) == 1
+    assert L.tk_set_variant(5, 0) == 1
+    tk.set_variant(tk.FORWARD, 1)
+    assert tk.get_variant(tk.FORWARD, 1000) == 1
+    tk.set_variant(tk.FORWARD, -1)
+    assert 0 <= tk.get_variant(tk.FORWARD, 1000) < tk.variant_count()
+    assert L.tk_get_variant(7, 10) < 0
+
+
+def test_get_table_sizes(tk):
+    L = tk.lib()
+    assert L.tk_get_table(0, None, 0) == 16 * 16 * 2
+    assert L.tk_get_table(1, None, 0) == 16 * 16 * 16 * 2
+    assert L.tk_get_table(6, None, 0) < 0
+    small = (ctypes.c_uint8 * 4)()
+    assert L.tk_get_table(0, small, 4) == 512                 # truncating copy is allowed

@@ -229,3 +229,21 @@ def test_large_batch_every_coefficient(tk, cuda, oracle):
     out = t.cpu().numpy()
     assert (canon(out) == canon(x.astype(np.int64) * 65536)).all()
     assert tk.device_status(0) == 0
+
+
+def test_reference_name_shims(tk, cuda, oracle):
+    """libtk_pqcrystals.so exports the reference's own symbol names
+    (ntt_bench/ref/ntt.h under KYBER_NAMESPACE) and matches the oracle mod q."""
+    import os
+    shim = ctypes.CDLL(os.path.join(os.path.dirname(tk.LIB_PATH), "libtk_pqcrystals.so"))
+    x = rng(31).integers(-3000, 3000, size=(3, 256)).astype(np.int16)
+    for k in ("512", "768", "1024"):
+        f = getattr(shim, f"pqcrystals_kyber{k}_ref_ntt")
+        g = getattr(shim, f"pqcrystals_kyber{k}_ref_invntt")
+        for i in range(3):
+            p = np.ascontiguousarray(x[i].copy())
+            f(p.ctypes.data)
+            assert shim.tk_pqcrystals_last_status() == 0
+            assert (p == canon(oracle.ntt(x[i:i + 1])[0])).all()
+            g(p.ctypes.data)
+            assert (canon(p) == canon(x[i].astype(np.int64) * 65536)).all()
