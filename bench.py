@@ -47,6 +47,10 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=6.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--variant", type=int, default=-1, help="force a kernel variant (-1: auto)")
+    p.add_argument("--sweep", action="store_true",
+                   help="batch-size sweep 2^0..2^sweep-max (autotuned), JSON lines to --sweep-out")
+    p.add_argument("--sweep-max", type=int, default=24)
+    p.add_argument("--sweep-out", default="sweep.jsonl")
     return p.parse_args()
 
 
@@ -321,9 +325,76 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_sweep(args):
+    """Batch-size sweep: for every power of two up to 2^sweep-max, forward,
+    inverse and round-trip throughput with the autotuned variant, as JSON lines
+    (one per size) in --sweep-out; the summary line goes to stdout."""
+    import torch
+
+    import tensorkyber_b200 as tk
+
+    torch.cuda.set_device(0)
+    tk.init(0)
+    t0 = time.perf_counter()
+    tk.autotune(max_npoly=1 << min(args.sweep_max, 22), device=0)
+    tune_s = time.perf_counter() - t0
+    peak, peak_kind = load_peak()
+    stream = torch.cuda.current_stream()
+    rows = []
+    with open(args.sweep_out, "w") as out:
+        for b in range(args.sweep_max + 1):
+            n = 1 << b
+            nb = 4 if 4 * n * 512 <= (40 << 30) else 2
+            batches = [torch.randint(0, Q, (n, 256), dtype=torch.int16, device="cuda")
+                       for _ in range(nb)]
+            # ~0.2 s of work per measurement, at least 20 launches
+            K = max(20, min(4000, int(0.1 / max(n * 1024 / (peak * 1e9 * 0.7), 6e-6))))
+            res = {}
+            for name, fns in (("fwd", (tk.ntt,)), ("inv", (tk.invntt,)),
+                              ("roundtrip", (tk.ntt, tk.invntt))):
+                for k in range(3):
+                    for f in fns:
+                        f(batches[k % nb], stream=stream)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                for k in range(K):
+                    for j, f in enumerate(fns):
+                        f(batches[(len(fns) * k + j) % nb], stream=stream)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                res[name] = e0.elapsed_time(e1) * 1e3 / K   # us per step
+            row = {
+                "npoly": n,
+                "fwd_us": res["fwd"], "inv_us": res["inv"], "roundtrip_us": res["roundtrip"],
+                "polys_per_s": n / (res["roundtrip"] * 1e-6),
+                "hbm_frac": (2 * n * 1024 / (res["roundtrip"] * 1e-6)) / (peak * 1e9),
+                "l2_resident": nb * n * 512 < (126 << 20),
+                "variant": {"fwd": tk.get_variant(tk.FORWARD, n),
+                            "inv": tk.get_variant(tk.INVERSE, n)},
+                "steps": K,
+            }
+            rows.append(row)
+            out.write(json.dumps(row) + "\n")
+            out.flush()
+            del batches
+            torch.cuda.empty_cache()
+    big = [r for r in rows if r["npoly"] >= (1 << 20)]
+    print(json.dumps({
+        "metric": "batch-size sweep NTT+iNTT polys/s and %HBM roofline (autotuned variants)",
+        "points": len(rows), "out": args.sweep_out, "autotune_s": tune_s,
+        "peak_gbs": peak, "peak_source": peak_kind,
+        "best_polys_per_s": max(r["polys_per_s"] for r in rows),
+        "min_hbm_frac_at_2^20_plus": min(r["hbm_frac"] for r in big) if big else None,
+    }), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.sweep:
+        run_sweep(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

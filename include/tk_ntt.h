@@ -100,6 +100,16 @@ const char *tk_variant_name(int variant);
 int tk_set_variant(int direction, int variant);
 int tk_get_variant(int direction, size_t npoly);
 
+/* Autotuner.  Times every variant in both directions at each power-of-two
+ * batch size 1 .. max_npoly on `device` (one scratch buffer of max_npoly
+ * polynomials is allocated and freed) and keeps the fastest per direction and
+ * size bucket floor(log2(npoly)) for all later calls; larger sizes use the
+ * largest tuned bucket.  With cache_path, a valid cache file is loaded instead
+ * of tuning, and a fresh tuning is written to it.  Synchronous.
+ * tk_autotune_reset() returns to the built-in choice. */
+int tk_autotune(int device, size_t max_npoly, const char *cache_path);
+int tk_autotune_reset(void);
+
 const char *tk_status_string(int status);
 /* Detail of the last failure on the calling thread ("" if none). */
 const char *tk_last_error(void);

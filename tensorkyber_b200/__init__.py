@@ -101,6 +101,9 @@ def lib() -> ctypes.CDLL:
     L.tk_set_variant.restype = ctypes.c_int
     L.tk_get_variant.argtypes = [ctypes.c_int, ctypes.c_size_t]
     L.tk_get_variant.restype = ctypes.c_int
+    L.tk_autotune.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.c_char_p]
+    L.tk_autotune.restype = ctypes.c_int
+    L.tk_autotune_reset.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -208,6 +211,15 @@ def set_variant(direction: int, variant: int) -> None:
 
 def get_variant(direction: int, npoly: int) -> int:
     return lib().tk_get_variant(direction, npoly)
+
+
+def autotune(max_npoly: int = 1 << 20, device: int = 0, cache_path: str | None = None) -> None:
+    """Pick the fastest kernel variant per direction and power-of-two size."""
+    _check(lib().tk_autotune(device, max_npoly, cache_path.encode() if cache_path else None))
+
+
+def autotune_reset() -> None:
+    lib().tk_autotune_reset()
 
 
 def init(device: int = 0) -> None:

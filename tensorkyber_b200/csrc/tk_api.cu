@@ -41,11 +41,28 @@ const char* const kVariantNames[tk::kNumMmaVariants] = {
     "mma.sync 4 warps x 32-poly tiles, 2-slot TMA ring",
 };
 
+// Autotuned choice per direction and size bucket floor(log2(npoly)); -1 =
+// not tuned (variant 0, the fastest shape measured at every large size).
+constexpr int kBuckets = 33;
+std::atomic<int> g_tuned[2][kBuckets];
+struct TunedInit {
+  TunedInit() {
+    for (auto& d : g_tuned)
+      for (auto& b : d) b.store(-1);
+  }
+} g_tuned_init;
+
+int size_bucket(size_t npoly) {
+  int b = 0;
+  while (b + 1 < kBuckets && ((size_t)1 << (b + 1)) <= npoly) b++;
+  return b;
+}
+
 int choose_variant(bool inverse, size_t npoly) {
   const int f = g_forced[inverse ? 1 : 0].load(std::memory_order_relaxed);
   if (f >= 0) return f;
-  (void)npoly;
-  return 0;
+  const int t = g_tuned[inverse ? 1 : 0][size_bucket(npoly)].load(std::memory_order_relaxed);
+  return t >= 0 ? t : 0;
 }
 
 void set_err(const char* what, cudaError_t e) {
@@ -342,6 +359,113 @@ int tk_get_variant(int direction, size_t npoly) {
   return choose_variant(direction == TK_INVERSE, npoly);
 }
 int tk_abi_version(void) { return TK_ABI_VERSION; }
+
+// ---- autotuner ----------------------------------------------------------------
+static int load_tuning(const char* path) {
+  FILE* f = fopen(path, "r");
+  if (!f) return TK_ERR_INVALID_VALUE;
+  char head[64] = {0};
+  int rc = TK_ERR_INVALID_VALUE;
+  if (fgets(head, sizeof(head), f) && strncmp(head, "tk-autotune 1", 13) == 0) {
+    int dir, bucket, variant;
+    double us;
+    int n = 0;
+    while (fscanf(f, "%d %d %d %lf", &dir, &bucket, &variant, &us) == 4) {
+      if (dir < 0 || dir > 1 || bucket < 0 || bucket >= kBuckets || variant < 0 ||
+          variant >= tk::kNumMmaVariants) {
+        n = -1;
+        break;
+      }
+      g_tuned[dir][bucket].store(variant);
+      n++;
+    }
+    rc = n > 0 ? TK_SUCCESS : TK_ERR_INVALID_VALUE;
+  }
+  fclose(f);
+  return rc;
+}
+
+int tk_autotune(int device, size_t max_npoly, const char* cache_path) {
+  t_err[0] = 0;
+  if (cache_path && load_tuning(cache_path) == TK_SUCCESS) return TK_SUCCESS;
+  if (max_npoly == 0 || max_npoly > TK_MAX_POLYS) {
+    set_msg("tk_autotune: max_npoly out of range");
+    return TK_ERR_INVALID_VALUE;
+  }
+  int rc = tk_init(device);
+  if (rc) return rc;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  DeviceInfo* info;
+  ensure_ready(device, &info);
+  int16_t* buf = nullptr;
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaMalloc(&buf, max_npoly * 512u);
+  if (e == cudaSuccess) e = cudaMemsetAsync(buf, 0, max_npoly * 512u);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  double best_us[2][kBuckets];
+  int best_v[2][kBuckets];
+  const int top = size_bucket(max_npoly);
+  for (int b = 0; b <= top && e == cudaSuccess; b++) {
+    const size_t n = (size_t)1 << b;
+    // enough launches per measurement for ~1 ms of work, at least 3
+    int reps = (int)((size_t)(1u << 21) / n);
+    reps = reps < 3 ? 3 : (reps > 200 ? 200 : reps);
+    for (int dir = 0; dir < 2 && e == cudaSuccess; dir++) {
+      best_us[dir][b] = 1e30;
+      best_v[dir][b] = 0;
+      for (int v = 0; v < tk::kNumMmaVariants && e == cudaSuccess; v++) {
+        for (int w = 0; w < 2 && e == cudaSuccess; w++)
+          e = tk::launch_mma(dir == 1, v, buf, buf, (long long)n, *info, st);
+        if (e == cudaSuccess) e = cudaEventRecord(e0, st);
+        for (int r = 0; r < reps && e == cudaSuccess; r++)
+          e = tk::launch_mma(dir == 1, v, buf, buf, (long long)n, *info, st);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        const double us = 1e3 * ms / reps;
+        if (e == cudaSuccess && us < best_us[dir][b]) {
+          best_us[dir][b] = us;
+          best_v[dir][b] = v;
+        }
+      }
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (st) cudaStreamDestroy(st);
+  if (buf) cudaFree(buf);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    set_err("tk_autotune", e);
+    return TK_ERR_CUDA;
+  }
+  // Buckets above the tuned range inherit the largest tuned one.
+  for (int dir = 0; dir < 2; dir++)
+    for (int b = 0; b < kBuckets; b++) g_tuned[dir][b].store(best_v[dir][b <= top ? b : top]);
+  if (cache_path) {
+    FILE* f = fopen(cache_path, "w");
+    if (f) {
+      fprintf(f, "tk-autotune 1\n");
+      for (int dir = 0; dir < 2; dir++)
+        for (int b = 0; b <= top; b++)
+          fprintf(f, "%d %d %d %.3f\n", dir, b, best_v[dir][b], best_us[dir][b]);
+      fclose(f);
+    }
+  }
+  return TK_SUCCESS;
+}
+
+int tk_autotune_reset(void) {
+  for (auto& d : g_tuned)
+    for (auto& b : d) b.store(-1);
+  return TK_SUCCESS;
+}
 
 long long tk_get_table(int which, void* out, size_t bytes) {
   static tk::Matrices M;

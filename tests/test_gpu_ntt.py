@@ -247,3 +247,23 @@ def test_reference_name_shims(tk, cuda, oracle):
             assert (p == canon(oracle.ntt(x[i:i + 1])[0])).all()
             g(p.ctypes.data)
             assert (canon(p) == canon(x[i].astype(np.int64) * 65536)).all()
+
+
+def test_autotune_small_range(tk, cuda, oracle, tmp_path):
+    """The autotuner picks a valid variant per size, writes/loads its cache,
+    and transforms stay exact afterwards."""
+    cache = str(tmp_path / "tune.txt")
+    try:
+        tk.autotune(max_npoly=1 << 12, device=0, cache_path=cache)
+        lines = open(cache).read().splitlines()
+        assert lines[0] == "tk-autotune 1" and len(lines) == 1 + 2 * 13
+        for n in (1, 100, 4096, 1 << 20):
+            for d in (tk.FORWARD, tk.INVERSE):
+                assert 0 <= tk.get_variant(d, n) < tk.variant_count()
+        tk.autotune_reset()
+        tk.autotune(max_npoly=1 << 12, device=0, cache_path=cache)   # loads the cache
+        x = rng(77).integers(-3000, 3000, size=(3000, 256)).astype(np.int16)
+        check_fwd(gpu_fwd(tk, cuda, x), oracle.ntt(x))
+        check_inv(gpu_inv(tk, cuda, x), oracle.invntt(x))
+    finally:
+        tk.autotune_reset()
