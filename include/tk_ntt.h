@@ -74,6 +74,39 @@ int tk_invntt_oop(const int16_t *in, int16_t *out, size_t npoly, tk_stream_t str
 int tk_ntt_host(int16_t *polys, size_t npoly);
 int tk_invntt_host(int16_t *polys, size_t npoly);
 
+/* ---- matrix-vector jobs (ML-KEM shape) ----------------------------------
+ * For every job and i < k:
+ *     out_i = invntt( sum_j basemul(A_ij, ntt(s_j)) ) + e_i       (mod q)
+ * i.e. the composition of the reference's ntt (ntt_bench/ref/ntt.c:80-95),
+ * basemul over the 128 coefficient pairs with +-zetas[64 + t/2]
+ * (ntt_bench/ref/ntt.c:139-146) and invntt (ntt_bench/ref/ntt.c:106-126),
+ * the product A^T r / A s of ML-KEM encryption and key generation.  The
+ * reference repository has no polyvec wrapper; this call has no direct
+ * counterpart there.  A is in the NTT domain; s, e any int16.  Output residues
+ * are exact mod q; the representative is the centred inverse output plus e
+ * (int16 wrap-around add, as the reference's polynomial add).
+ * Jobs of one batch share k and are packed: job t uses A[t*k*k .. ),
+ * s/e/out[t*k .. ).  Mixed ML-KEM-512/768/1024 work is one call with up to
+ * three batches.  All buffers are device memory, 16-byte aligned; out may be
+ * s itself but must not overlap A or e; e may be NULL.  Asynchronous on
+ * stream; makes no allocation; capturable in a CUDA graph after tk_init. */
+typedef struct tk_matvec_batch {
+  int k;
+  size_t njobs;
+  const int16_t *A;
+  const int16_t *s;
+  const int16_t *e;
+  int16_t *out;
+} tk_matvec_batch;
+int tk_matvec(const tk_matvec_batch *batches, int nbatches, tk_stream_t stream);
+
+/* ---- process-wide options ---------------------------------------------------
+ * TK_OPT_MATVEC_CHUNK_POLYS: vector polynomials per tk_matvec chunk (the
+ * chunk's intermediates are meant to stay in L2); 0 restores the default. */
+#define TK_OPT_MATVEC_CHUNK_POLYS 1
+int tk_set_option(int option, long long value);
+long long tk_get_option(int option);
+
 /* ---- runtime --------------------------------------------------------------
  * tk_init: per-device set-up (constant tables, occupancy).  Every entry point
  * runs it on first use of a device; call it explicitly before capturing a

@@ -31,6 +31,12 @@ STATUS = {
 }
 
 
+class MatvecBatch(ctypes.Structure):
+    """Mirror of tk_matvec_batch (include/tk_ntt.h)."""
+    _fields_ = [("k", ctypes.c_int), ("njobs", ctypes.c_size_t), ("A", ctypes.c_void_p),
+                ("s", ctypes.c_void_p), ("e", ctypes.c_void_p), ("out", ctypes.c_void_p)]
+
+
 class TKError(RuntimeError):
     def __init__(self, status: int, detail: str = ""):
         self.status = status
@@ -104,6 +110,12 @@ def lib() -> ctypes.CDLL:
     L.tk_autotune.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.c_char_p]
     L.tk_autotune.restype = ctypes.c_int
     L.tk_autotune_reset.restype = ctypes.c_int
+    L.tk_matvec.argtypes = [ctypes.POINTER(MatvecBatch), ctypes.c_int, ctypes.c_void_p]
+    L.tk_matvec.restype = ctypes.c_int
+    L.tk_set_option.argtypes = [ctypes.c_int, ctypes.c_longlong]
+    L.tk_set_option.restype = ctypes.c_int
+    L.tk_get_option.argtypes = [ctypes.c_int]
+    L.tk_get_option.restype = ctypes.c_longlong
     _lib = L
     return L
 
@@ -191,6 +203,35 @@ def invntt_host(a: np.ndarray) -> np.ndarray:
     """Inverse NTT of host polynomials in place (synchronous, through the GPU)."""
     _check(lib().tk_invntt_host(a.ctypes.data, _host_arr(a)))
     return a
+
+
+def matvec(batches, stream=None):
+    """ML-KEM matrix-vector jobs on CUDA int16 tensors.
+
+    batches: iterable of (k, A, s, e, out) with A of shape (njobs, k, k, 256),
+    s / e / out of shape (njobs, k, 256); e may be None; out may be s.
+    out_i = invntt(sum_j basemul(A_ij, ntt(s_j))) + e_i for every job."""
+    items = []
+    for k, A, s, e, out in batches:
+        n = _check_tensor(s) // k
+        if _check_tensor(A) != n * k * k or _check_tensor(out) != n * k or (
+                e is not None and _check_tensor(e) != n * k):
+            raise ValueError("inconsistent matvec batch shapes")
+        items.append(MatvecBatch(k, n, A.data_ptr(), s.data_ptr(),
+                                 e.data_ptr() if e is not None else None, out.data_ptr()))
+    arr = (MatvecBatch * len(items))(*items)
+    _check(lib().tk_matvec(arr, len(items), _stream_ptr(stream)))
+
+
+OPT_MATVEC_CHUNK_POLYS = 1
+
+
+def set_option(option: int, value: int) -> None:
+    _check(lib().tk_set_option(option, value))
+
+
+def get_option(option: int) -> int:
+    return lib().tk_get_option(option)
 
 
 FORWARD, INVERSE = 0, 1

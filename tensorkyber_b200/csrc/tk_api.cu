@@ -34,6 +34,7 @@ thread_local char t_err[256] = "";
 
 // Kernel variant choice: forced by tk_set_variant (>= 0) or picked by size.
 std::atomic<int> g_forced[2] = {{-1}, {-1}};
+std::atomic<long long> g_matvec_chunk{tk::kMatvecChunkVecPolys};
 
 const char* const kVariantNames[tk::kNumMmaVariants] = {
     "mma.sync 4 warps x 32-poly tiles, 3-slot TMA ring",
@@ -125,7 +126,7 @@ int ensure_ready(int dev, DeviceInfo** out) {
     S.info.cc_major = p.major;
     S.info.cc_minor = p.minor;
     S.info.total_mem = p.totalGlobalMem;
-    if (!tk::mma_init_device(&S.info)) {
+    if (!tk::mma_init_device(&S.info) || !tk::matvec_init_device()) {
       set_err("kernel set-up", cudaGetLastError());
       return TK_ERR_CUDA;
     }
@@ -273,6 +274,74 @@ int tk_invntt_oop(const int16_t* in, int16_t* out, size_t npoly, tk_stream_t str
   return run_device(true, in, out, npoly, (cudaStream_t)stream);
 }
 int tk_ntt_host(int16_t* polys, size_t npoly) { return run_host(false, polys, npoly); }
+
+static bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+  const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+  return x < y + nb && y < x + na;
+}
+
+int tk_matvec(const tk_matvec_batch* batches, int nbatches, tk_stream_t stream) {
+  t_err[0] = 0;
+  if (nbatches < 0 || (nbatches > 0 && !batches)) {
+    set_msg("tk_matvec: bad batch list");
+    return TK_ERR_INVALID_VALUE;
+  }
+  int nonempty = 0;
+  for (int b = 0; b < nbatches; b++) {  // validate everything before launching anything
+    const tk_matvec_batch& B = batches[b];
+    if (B.njobs == 0) continue;
+    nonempty++;
+    if (B.k < 2 || B.k > 4) {
+      set_msg("tk_matvec: k must be 2, 3 or 4");
+      return TK_ERR_INVALID_VALUE;
+    }
+    if (!B.A || !B.s || !B.out) {
+      set_msg("tk_matvec: NULL A, s or out");
+      return TK_ERR_INVALID_VALUE;
+    }
+    if (B.njobs > ((size_t)1 << 28)) {
+      set_msg("tk_matvec: too many jobs in one batch");
+      return TK_ERR_TOO_LARGE;
+    }
+    if ((((uintptr_t)B.A | (uintptr_t)B.s | (uintptr_t)B.e | (uintptr_t)B.out) & 15u) != 0) {
+      set_msg("tk_matvec: buffers must be 16-byte aligned");
+      return TK_ERR_MISALIGNED;
+    }
+    const size_t vb = B.njobs * (size_t)B.k * 512u, ab = vb * (size_t)B.k;
+    if (overlaps(B.out, vb, B.A, ab) || (B.e && overlaps(B.out, vb, B.e, vb)) ||
+        (B.s != B.out && overlaps(B.out, vb, B.s, vb))) {
+      set_msg("tk_matvec: out overlaps A or e, or partially overlaps s");
+      return TK_ERR_INVALID_VALUE;
+    }
+  }
+  if (nonempty == 0) return TK_SUCCESS;
+  int dev;
+  int rc = current_device(&dev);
+  if (rc) return rc;
+  DeviceInfo* info;
+  rc = ensure_ready(dev, &info);
+  if (rc) return rc;
+  for (int b = 0; b < nbatches; b++) {
+    const tk_matvec_batch& B = batches[b];
+    if (B.njobs == 0) continue;
+    const void* ptrs[4] = {B.A, B.s, B.out, B.e};
+    for (const void* p : ptrs)
+      if (p && (rc = check_device_ptr(p))) return rc;
+  }
+  for (int b = 0; b < nbatches; b++) {
+    const tk_matvec_batch& B = batches[b];
+    if (B.njobs == 0) continue;
+    const long long chunk = g_matvec_chunk.load(std::memory_order_relaxed);
+    cudaError_t e = tk::launch_matvec(B.k, B.njobs, B.A, B.s, B.e, B.out, *info,
+                                      (cudaStream_t)stream, choose_variant(false, (size_t)chunk),
+                                      choose_variant(true, (size_t)chunk), chunk);
+    if (e != cudaSuccess) {
+      set_launch_err(e);
+      return TK_ERR_CUDA;
+    }
+  }
+  return TK_SUCCESS;
+}
 int tk_invntt_host(int16_t* polys, size_t npoly) { return run_host(true, polys, npoly); }
 
 int tk_init(int device) {
@@ -352,6 +421,27 @@ int tk_set_variant(int direction, int variant) {
   }
   g_forced[direction == TK_INVERSE ? 1 : 0].store(variant);
   return TK_SUCCESS;
+}
+
+int tk_set_option(int option, long long value) {
+  t_err[0] = 0;
+  switch (option) {
+    case TK_OPT_MATVEC_CHUNK_POLYS:
+      if (value < 0 || value > (1ll << 30)) break;
+      g_matvec_chunk.store(value == 0 ? tk::kMatvecChunkVecPolys : value);
+      return TK_SUCCESS;
+    default:
+      break;
+  }
+  set_msg("tk_set_option: unknown option or value out of range");
+  return TK_ERR_INVALID_VALUE;
+}
+
+long long tk_get_option(int option) {
+  switch (option) {
+    case TK_OPT_MATVEC_CHUNK_POLYS: return g_matvec_chunk.load();
+    default: return -TK_ERR_INVALID_VALUE;
+  }
 }
 
 int tk_get_variant(int direction, size_t npoly) {

@@ -27,12 +27,24 @@ struct DeviceInfo {
 bool mma_init_device(DeviceInfo* info);
 
 // Batched transform of npoly polynomials, src -> dst (src == dst for in place).
+// Inverse only: a non-null addend (npoly polynomials) is added to the output
+// with int16 wrap-around.
 cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* dst,
-                       long long npoly, const DeviceInfo& info, cudaStream_t stream);
+                       long long npoly, const DeviceInfo& info, cudaStream_t stream,
+                       const int16_t* addend = nullptr);
 
 // CUresult of the calling thread's last tensor-map encode (launch_mma reports
 // cudaErrorInvalidResourceHandle when an encode failed).
 int last_encode_result();
+
+// Matrix-vector jobs (tk_matvec.cu).  Chunks hold at most this many vector
+// polynomials, so that intermediates stay in the 126 MB L2.
+constexpr long long kMatvecChunkVecPolys = 131072;  // default (64 MiB); tk_set_option may change it
+bool matvec_init_device();
+cudaError_t launch_matvec(int k, size_t njobs, const int16_t* A, const int16_t* s,
+                          const int16_t* e, int16_t* out, const DeviceInfo& info,
+                          cudaStream_t stream, int fwd_variant, int inv_variant,
+                          long long chunk_vec_polys);
 
 // Kernel-side error flags (bounded waits that gave up), read and reset.
 cudaError_t read_and_clear_status(unsigned* flags);

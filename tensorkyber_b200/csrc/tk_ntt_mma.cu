@@ -85,7 +85,7 @@ template <bool kInverse>
 __device__ __forceinline__ void stage_m(const uint32_t (&a)[2][4], int32_t c_lo, int32_t c_hi,
                                         uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3,
                                         uint8_t* row, uint32_t w_even, uint32_t w_odd,
-                                        uint32_t w_nat) {
+                                        uint32_t w_nat, const uint32_t (&add)[4]) {
   const int32_t cinit[4] = {c_lo, c_lo, c_hi, c_hi};
   const int32_t zero[4] = {0, 0, 0, 0};
   int32_t lo0[4], hi0[4], lo1[4], hi1[4];
@@ -107,7 +107,15 @@ __device__ __forceinline__ void stage_m(const uint32_t (&a)[2][4], int32_t c_lo,
     }
   }
   // D regs: [0] (row i, c=2q), [1] (row i, c=2q+1), [2]/[3] row i+8; n-tile 1 is c+8.
-  if (kInverse) {  // natural order
+  if (kInverse) {  // natural order; plus the addend pairs (int16 wrap-around add)
+    y0[0] += (uint32_t)(int32_t)(int16_t)(add[0] & 0xffffu);
+    y0[1] += (uint32_t)((int32_t)add[0] >> 16);
+    y1[0] += (uint32_t)(int32_t)(int16_t)(add[1] & 0xffffu);
+    y1[1] += (uint32_t)((int32_t)add[1] >> 16);
+    y0[2] += (uint32_t)(int32_t)(int16_t)(add[2] & 0xffffu);
+    y0[3] += (uint32_t)((int32_t)add[2] >> 16);
+    y1[2] += (uint32_t)(int32_t)(int16_t)(add[3] & 0xffffu);
+    y1[3] += (uint32_t)((int32_t)add[3] >> 16);
     *(uint32_t*)(row + w_nat) = pack2(y0[0], y0[1]);
     *(uint32_t*)(row + w_nat + 16) = pack2(y1[0], y1[1]);
     *(uint32_t*)(row + w_nat + 256) = pack2(y0[2], y0[3]);
@@ -191,26 +199,49 @@ __device__ __forceinline__ void block_stage(uint32_t slot, uint8_t* slotp, int b
 }
 
 // Stage over m for this warp's 8 polynomials, the next ldmatrix issued ahead.
+// Inverse only: with an addend, polynomial p of this warp (global index
+// poly0 + p) gets addend[poly0 + p] added to its output; the addend words for
+// polynomial p+1 are fetched while p is computed.
 template <bool kInverse>
 __device__ __forceinline__ void poly_stage(uint32_t mine, uint8_t* minep, uint32_t ldt_off,
                                            const uint32_t (&am)[2][4], int32_t cm_lo,
                                            int32_t cm_hi, uint32_t w_even, uint32_t w_odd,
-                                           uint32_t w_nat) {
-  uint32_t b[4];
+                                           uint32_t w_nat, const uint32_t* addend, int poly0,
+                                           int npoly, uint32_t add_off) {
+  auto load_add = [&](int p, uint32_t (&e)[4]) {
+    const int poly = poly0 + p;
+    if (kInverse && addend != nullptr && poly < npoly) {
+      const uint32_t* w = addend + (size_t)poly * 128 + add_off;
+      e[0] = __ldg(w);
+      e[1] = __ldg(w + 4);
+      e[2] = __ldg(w + 64);
+      e[3] = __ldg(w + 68);
+    } else {
+      e[0] = e[1] = e[2] = e[3] = 0;
+    }
+  };
+  uint32_t b[4], e[4];
   ldsm_x4_t(mine + ldt_off, b[0], b[1], b[2], b[3]);
+  load_add(0, e);
 #pragma unroll
   for (int p = 0; p < 8; p++) {
-    uint32_t n[4] = {0, 0, 0, 0};
-    if (p < 7) ldsm_x4_t(mine + (p + 1) * kRowBytes + ldt_off, n[0], n[1], n[2], n[3]);
+    uint32_t n[4] = {0, 0, 0, 0}, en[4] = {0, 0, 0, 0};
+    if (p < 7) {
+      ldsm_x4_t(mine + (p + 1) * kRowBytes + ldt_off, n[0], n[1], n[2], n[3]);
+      load_add(p + 1, en);
+    }
     if (kInverse)
       stage_m<true>(am, cm_lo, cm_hi, b[0], b[1], b[2], b[3], minep + p * kRowBytes, 0, 0,
-                    w_nat);
+                    w_nat, e);
     else  // x ^ 0x8000 bias; the 32768 * rowsum term is cancelled by cm_lo/cm_hi
       stage_m<false>(am, cm_lo, cm_hi, b[0] ^ 0x80008000u, b[1] ^ 0x80008000u,
                      b[2] ^ 0x80008000u, b[3] ^ 0x80008000u, minep + p * kRowBytes, w_even,
-                     w_odd, 0);
+                     w_odd, 0, e);
 #pragma unroll
-    for (int j = 0; j < 4; j++) b[j] = n[j];
+    for (int j = 0; j < 4; j++) {
+      b[j] = n[j];
+      e[j] = en[j];
+    }
   }
 }
 
@@ -218,7 +249,7 @@ __device__ __forceinline__ void poly_stage(uint32_t mine, uint8_t* minep, uint32
 template <bool kInverse, int W, int S>
 __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
     k_ntt_mma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_out,
-              int npoly) {
+              int npoly, const uint32_t* __restrict__ addend) {
   using C = Cfg<W, S>;
   extern __shared__ __align__(128) uint8_t smem[];
   const int tid = threadIdx.x;
@@ -335,7 +366,8 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
     uint8_t* minep = slotp + 8 * warp * kRowBytes;
 
     if (!kInverse) {
-      poly_stage<false>(mine, minep, ldt_off, am, cm_lo, cm_hi, w_even, w_odd, 0);
+      poly_stage<false>(mine, minep, ldt_off, am, cm_lo, cm_hi, w_even, w_odd, 0, nullptr, 0, 0,
+                        0);
       cta_sync_named();
       block_stage<false, W>(slot, slotp, blk0, ldc_off, stc_off, ac, cc);
       fence_proxy_async_smem();
@@ -344,7 +376,8 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
     } else {
       block_stage<true, W>(slot, slotp, blk0, ldc_off, stc_off, ac, cc);
       cta_sync_named();
-      poly_stage<true>(mine, minep, ldt_off, am, cm_lo, cm_hi, 0, 0, w_nat);
+      poly_stage<true>(mine, minep, ldt_off, am, cm_lo, cm_hi, 0, 0, w_nat, addend,
+                       8 * (u_begin + k * W + warp), npoly, 8u * g8 + q4);
       fence_proxy_async_smem();
       __syncwarp();
       issue_store(k, slot_i);
@@ -358,7 +391,7 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
 }
 
 // ------------------------------------------------------------ host side ----
-using Fn = void (*)(const CUtensorMap, const CUtensorMap, int);
+using Fn = void (*)(const CUtensorMap, const CUtensorMap, int, const uint32_t*);
 
 struct Variant {
   Fn fn;
@@ -450,7 +483,8 @@ bool mma_init_device(DeviceInfo* info) {
 }
 
 cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* dst,
-                       long long npoly, const DeviceInfo& info, cudaStream_t stream) {
+                       long long npoly, const DeviceInfo& info, cudaStream_t stream,
+                       const int16_t* addend) {
   if (variant < 0 || variant >= kNumMmaVariants) variant = 0;
   const Variant& V = kVariants[inverse ? 1 : 0][variant];
   const long long cap = (long long)info.num_sms * info.mma_ctas_per_sm[inverse ? 1 : 0][variant];
@@ -476,7 +510,8 @@ cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* d
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const cudaError_t e = cudaLaunchKernelEx(&cfg, V.fn, m_in, m_out, n);
+    const uint32_t* add = addend ? (const uint32_t*)(addend + done * 256) : nullptr;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, V.fn, m_in, m_out, n, add);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

@@ -88,3 +88,23 @@ def test_get_table_sizes(tk):
     assert L.tk_get_table(6, None, 0) < 0
     small = (ctypes.c_uint8 * 4)()
     assert L.tk_get_table(0, small, 4) == 512                 # truncating copy is allowed
+
+
+def test_matvec_argument_errors_without_gpu(tk):
+    L = tk.lib()
+    buf = np.zeros(64 * 256 + 16, dtype=np.int16)
+    base = (buf.ctypes.data + 15) & ~15
+    B = tk.MatvecBatch
+    assert L.tk_matvec(None, 0, None) == 0
+    assert L.tk_matvec(None, 2, None) == 1
+    for k, expect in ((1, 1), (5, 1)):
+        arr = (B * 1)(B(k, 2, base, base + 8192, None, base + 16384))
+        assert L.tk_matvec(arr, 1, None) == expect
+    arr = (B * 1)(B(2, 2, None, base, None, base))
+    assert L.tk_matvec(arr, 1, None) == 1
+    arr = (B * 1)(B(2, 2, base + 2, base + 8192, None, base + 16384))
+    assert L.tk_matvec(arr, 1, None) == 2
+    arr = (B * 1)(B(2, 2, base, base + 8192, None, base + 512))      # out inside A
+    assert L.tk_matvec(arr, 1, None) == 1
+    arr = (B * 1)(B(2, 0, None, None, None, None))                  # empty batch: no-op
+    assert L.tk_matvec(arr, 1, None) == 0

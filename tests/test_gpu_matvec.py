@@ -1,0 +1,87 @@
+"""GPU parity of the ML-KEM matrix-vector jobs (tk_matvec) against the oracle's
+composition of the reference's ntt / basemul / invntt (tko_matvec_job).
+Integer work: every output coefficient must agree mod q."""
+import numpy as np
+import pytest
+
+from conftest import rng
+from py_oracle import Q, canon
+
+pytestmark = pytest.mark.gpu
+
+
+def make_jobs(seed, k, n, a_lo=0, a_hi=Q, small=3):
+    r = rng(seed)
+    A = r.integers(a_lo, a_hi, size=(n, k, k, 256)).astype(np.int16)
+    s = r.integers(-small, small + 1, size=(n, k, 256)).astype(np.int16)
+    e = r.integers(-small, small + 1, size=(n, k, 256)).astype(np.int16)
+    return A, s, e
+
+
+def oracle_out(oracle, k, A, s, e):
+    return np.stack([oracle.matvec_job(k, A[t].reshape(k * k, 256), s[t],
+                                       e[t] if e is not None else np.zeros_like(s[t]))
+                     for t in range(A.shape[0])])
+
+
+def run(tk, cuda, items, inplace=False):
+    dev = []
+    for k, A, s, e in items:
+        tA, ts = cuda.from_numpy(A).cuda(), cuda.from_numpy(s).cuda()
+        te = cuda.from_numpy(e).cuda() if e is not None else None
+        out = ts if inplace else cuda.empty_like(ts)
+        dev.append((k, tA, ts, te, out))
+    tk.matvec(dev)
+    cuda.cuda.synchronize()
+    return [d[4].cpu().numpy() for d in dev]
+
+
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_matvec_each_k(tk, cuda, oracle, k):
+    A, s, e = make_jobs(k, k, 203)
+    (out,) = run(tk, cuda, [(k, A, s, e)])
+    assert (canon(out) == canon(oracle_out(oracle, k, A, s, e))).all()
+
+
+def test_matvec_mixed_batches_one_call(tk, cuda, oracle):
+    items = [(k,) + make_jobs(10 + k, k, n) for k, n in ((3, 77), (2, 130), (4, 51))]
+    outs = run(tk, cuda, items)
+    for (k, A, s, e), out in zip(items, outs):
+        assert (canon(out) == canon(oracle_out(oracle, k, A, s, e))).all()
+
+
+def test_matvec_no_addend_in_place_and_wide_inputs(tk, cuda, oracle):
+    """e = NULL, out == s, A over (-q, q) and s over the full int16 range."""
+    k = 3
+    A, s, _ = make_jobs(21, k, 64, a_lo=-Q + 1, a_hi=Q)
+    s_wide = rng(22).integers(-32768, 32768, size=s.shape).astype(np.int16)
+    (out,) = run(tk, cuda, [(k, A, s_wide, None)], inplace=True)
+    # the oracle's ntt overflows int16 outside |x| <= 9471: feed it canon(s)
+    ref = oracle_out(oracle, k, A, canon(s_wide).astype(np.int16), None)
+    assert (canon(out) == canon(ref)).all()
+
+
+def test_matvec_spans_several_chunks(tk, cuda, oracle):
+    """k = 2 with more jobs than one L2-sized chunk (16384 jobs for k = 2)."""
+    k, n = 2, 40000
+    A, s, e = make_jobs(31, k, n)
+    (out,) = run(tk, cuda, [(k, A, s, e)])
+    pick = np.r_[0:50, 16380:16390, n - 50:n]
+    assert (canon(out[pick]) == canon(oracle_out(oracle, k, A[pick], s[pick], e[pick]))).all()
+    assert tk.device_status(0) == 0
+
+
+def test_matvec_rejects_bad_batches(tk, cuda):
+    import ctypes
+    t = cuda.zeros((4, 2, 256), dtype=cuda.int16, device="cuda")
+    A = cuda.zeros((4, 2, 2, 256), dtype=cuda.int16, device="cuda")
+    L = tk.lib()
+    bad_k = (tk.MatvecBatch * 1)(tk.MatvecBatch(5, 4, A.data_ptr(), t.data_ptr(), None, t.data_ptr()))
+    assert L.tk_matvec(bad_k, 1, None) == 1
+    overlap = (tk.MatvecBatch * 1)(tk.MatvecBatch(2, 4, A.data_ptr(), t.data_ptr(), None, A.data_ptr()))
+    assert L.tk_matvec(overlap, 1, None) == 1
+    mis = (tk.MatvecBatch * 1)(tk.MatvecBatch(2, 4, A.data_ptr() + 2, t.data_ptr(), None, t.data_ptr()))
+    assert L.tk_matvec(mis, 1, None) == 2
+    assert L.tk_matvec(None, 0, None) == 0
+    assert L.tk_matvec(None, 1, None) == 1
+    del ctypes
