@@ -55,6 +55,13 @@ def parse():
                    help="fused ML-KEM matrix-vector jobs, k ~ U{2,3,4} (eager and CUDA graph)")
     p.add_argument("--jobs", type=int, default=65536)
     p.add_argument("--chunk", type=int, default=0, help="tk_matvec chunk (vector polys), 0 = default")
+    p.add_argument("--matvec-mode", type=int, default=0, help="0 pipeline, 1 fused single launch")
+    p.add_argument("--serve", action="store_true",
+                   help="serving loop: Poisson arrivals at swept rates, server vs plain per-request")
+    p.add_argument("--serve-requests", type=int, default=3000, help="requests per rate point")
+    p.add_argument("--serve-rates", default="0.25,0.5,0.9,1.5,3,6",
+                   help="offered load as multiples of the plain per-request capacity")
+    p.add_argument("--serve-templates", type=int, default=256)
     return p.parse_args()
 
 
@@ -407,6 +414,7 @@ def run_matvec(args):
     torch.cuda.set_device(0)
     tk.init(0)
     tk.set_option(tk.OPT_MATVEC_CHUNK_POLYS, args.chunk)
+    tk.set_option(tk.OPT_MATVEC_MODE, args.matvec_mode)
     ks = np.random.default_rng(2024).integers(2, 5, size=args.jobs)
     g = torch.Generator(device="cuda").manual_seed(7)
     batches, nbytes = [], 0
@@ -459,7 +467,8 @@ def run_matvec(args):
         "eager_ms_per_step": eager_ms, "eager_jobs_per_s": args.jobs / (eager_ms * 1e-3),
         "jobs_per_k": {str(k): int((ks == k).sum()) for k in (2, 3, 4)},
         "config": {"workload": f"{args.jobs} jobs, A k x k uniform [0,q) NTT domain, s,e in [-3,3]",
-                   "chunk_vec_polys": tk.get_option(tk.OPT_MATVEC_CHUNK_POLYS)},
+                   "chunk_vec_polys": tk.get_option(tk.OPT_MATVEC_CHUNK_POLYS),
+                   "mode": ["pipeline", "fused"][tk.get_option(tk.OPT_MATVEC_MODE)]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "bytes_per_step": nbytes,
                      "peak_source": peak_kind},
@@ -467,9 +476,149 @@ def run_matvec(args):
     }), flush=True)
 
 
+def run_serve(args):
+    """Serving loop against the plain per-request launch, on the same requests.
+
+    A request is njobs ~ U{1..64} matrix-vector jobs of one k ~ U{2,3,4} with
+    every coefficient uniform in [0, q) (seeded), in pinned host memory.
+    Arrivals are Poisson at a rate swept as multiples of the plain path's
+    measured capacity.  Plain: one host thread serves requests in arrival
+    order, each as tk_matvec_host (copy in, one fused launch, copy out, sync).
+    Server: the same thread submits each request at its arrival time to
+    tk_server (continuous batching).  Latency = completion - scheduled
+    arrival; throughput = output polynomials / (last completion - start)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import tensorkyber_b200 as tk
+
+    torch.cuda.set_device(0)
+    tk.init(0)
+    tk.set_option(tk.OPT_MATVEC_MODE, tk.MATVEC_FUSED)
+    L = tk.lib()
+    r = np.random.default_rng(2025)
+    T = args.serve_templates
+
+    def pinned(shape):
+        return torch.empty(shape, dtype=torch.int16, pin_memory=True).numpy()
+
+    tmpl = []
+    for _ in range(T):
+        k, n = int(r.integers(2, 5)), int(r.integers(1, 65))
+        A, sv, e = pinned((n, k, k, 256)), pinned((n, k, 256)), pinned((n, k, 256))
+        A[...] = r.integers(0, Q, size=A.shape)
+        sv[...] = r.integers(0, Q, size=sv.shape)
+        e[...] = r.integers(0, Q, size=e.shape)
+        o_plain, o_srv = pinned((n, k, 256)), pinned((n, k, 256))
+        batch = (tk.MatvecBatch * 1)(tk.MatvecBatch(k, n, A.ctypes.data, sv.ctypes.data,
+                                                    e.ctypes.data, o_plain.ctypes.data))
+        tmpl.append(dict(k=k, n=n, A=A, s=sv, e=e, o_plain=o_plain, o_srv=o_srv, batch=batch,
+                         ptrs=(A.ctypes.data, sv.ctypes.data, e.ctypes.data, o_srv.ctypes.data)))
+    polys = np.array([t["n"] * t["k"] for t in tmpl])
+    pc = time.perf_counter
+
+    def plain_one(t):
+        rc = L.tk_matvec_host(t["batch"], 1)
+        if rc:
+            raise tk.TKError(rc, L.tk_last_error().decode())
+
+    for t in tmpl:                      # warm-up, reference outputs
+        plain_one(t)
+    t0 = pc()
+    for t in tmpl:
+        plain_one(t)
+    service = (pc() - t0) / T
+    cap = 1.0 / service
+
+    def spin_until(x):
+        while pc() < x:
+            pass
+
+    def pct(v, p):
+        return float(np.percentile(np.asarray(v) * 1e6, p))
+
+    srv = tk.Server(hbm_budget_bytes=1 << 30, max_inflight_requests=1024, idle_exit_seconds=0.05)
+    ticket = ctypes.c_uint64()
+    for t in tmpl:                      # server warm-up
+        a, b_, c, d = t["ptrs"]
+        if L.tk_server_submit(srv._h, t["k"], t["n"], a, b_, c, d, ctypes.byref(ticket)):
+            raise tk.TKError(1, "submit")
+        srv.wait(ticket.value)
+        srv.release(ticket.value)
+    points = []
+    sampler = ClockSampler(0)
+    sampler.start()
+    for mult in [float(x) for x in args.serve_rates.split(",")]:
+        rate = mult * cap
+        nreq = args.serve_requests
+        arr = np.cumsum(r.exponential(1.0 / rate, size=nreq))
+        which = r.integers(0, T, size=nreq)
+        tot_polys = int(polys[which].sum())
+        # plain per-request launch, FIFO
+        lat = np.empty(nreq)
+        base = pc() + 1e-3
+        for i in range(nreq):
+            ta = base + arr[i]
+            spin_until(ta)
+            plain_one(tmpl[which[i]])
+            lat[i] = pc() - ta
+        plain_end = max(base + arr[i] + lat[i] for i in range(nreq))
+        plain = {"p50_us": pct(lat, 50), "p99_us": pct(lat, 99),
+                 "polys_per_s": tot_polys / (plain_end - base),
+                 "requests_per_s": nreq / (plain_end - base)}
+        # server
+        lag = np.empty(nreq)
+        tickets = np.empty(nreq, dtype=np.uint64)
+        base = pc() + 1e-3
+        for i in range(nreq):
+            ta = base + arr[i]
+            spin_until(ta)
+            t = tmpl[which[i]]
+            a, b_, c, d = t["ptrs"]
+            rc = L.tk_server_submit(srv._h, t["k"], t["n"], a, b_, c, d, ctypes.byref(ticket))
+            lag[i] = pc() - ta
+            if rc:
+                raise tk.TKError(rc, "submit")
+            tickets[i] = ticket.value
+        slat = np.empty(nreq)
+        for i in range(nreq):
+            srv.wait(int(tickets[i]), timeout=60)
+            slat[i] = lag[i] + srv.latency(int(tickets[i]))
+            srv.release(int(tickets[i]))
+        srv_end = base + max(arr[i] + slat[i] for i in range(nreq))
+        server = {"p50_us": pct(slat, 50), "p99_us": pct(slat, 99),
+                  "polys_per_s": tot_polys / (srv_end - base),
+                  "requests_per_s": nreq / (srv_end - base),
+                  "submit_lag_p99_us": pct(lag, 99)}
+        points.append({"offered_x_plain_capacity": mult, "offered_requests_per_s": rate,
+                       "requests": nreq, "polys": tot_polys, "plain": plain, "server": server})
+    clocks = sampler.stop()
+    stats = srv.stats()
+    srv.close()
+    exact = all((t["o_srv"] == t["o_plain"]).all() for t in tmpl)
+    assert tk.device_status(0) == 0
+    top = points[-1]
+    print(json.dumps({
+        "metric": "serving: p50/p99 request latency (us) and polys/s under Poisson arrivals, 1xB200",
+        "value": top["server"]["polys_per_s"], "unit": "polys/s", "n_gpus": 1,
+        "higher_is_better": True,
+        "plain_service_us": service * 1e6, "plain_capacity_requests_per_s": cap,
+        "points": points, "server_outputs_equal_plain": bool(exact),
+        "server_stats": stats, "clocks": clocks,
+        "config": {"workload": "requests of 1-64 matrix-vector jobs, k ~ U{2,3,4}, "
+                               "coefficients uniform [0,q), pinned host buffers",
+                   "templates": T, "mode": "fused"},
+        "dtype": "int16", "data": "synthetic",
+    }), flush=True)
+
+
 def main():
     args = parse()
-    if args.matvec:
+    if args.serve:
+        run_serve(args)
+    elif args.matvec:
         run_matvec(args)
     elif args.sweep:
         run_sweep(args)

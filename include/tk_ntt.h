@@ -49,7 +49,8 @@ typedef enum tk_status {
   TK_ERR_NO_DEVICE = 4,          /* no CUDA device, or not an sm_100 (B200-class) GPU */
   TK_ERR_CUDA = 5,               /* a CUDA runtime call failed; tk_last_error() has the text */
   TK_ERR_NOT_DEVICE_MEMORY = 6,  /* device entry point given a pointer the GPU cannot address */
-  TK_ERR_KERNEL_TIMEOUT = 7      /* a kernel's bounded wait gave up (see tk_device_status) */
+  TK_ERR_KERNEL_TIMEOUT = 7,     /* a kernel's bounded wait gave up (see tk_device_status) */
+  TK_ERR_TIMEOUT = 8             /* a host-side wait reached its time limit */
 } tk_status;
 
 #define TK_MAX_POLYS ((size_t)1 << 32)
@@ -99,11 +100,53 @@ typedef struct tk_matvec_batch {
   int16_t *out;
 } tk_matvec_batch;
 int tk_matvec(const tk_matvec_batch *batches, int nbatches, tk_stream_t stream);
+/* tk_matvec on HOST buffers, synchronous: copies A, s, e in, runs the same
+ * kernels, copies out back (the plain per-request launch).  Uses a device
+ * staging buffer per device that grows to the largest call (at most 8 GiB);
+ * calls on one device are serialised.  out may alias s. */
+int tk_matvec_host(const tk_matvec_batch *batches, int nbatches);
+
+/* ---- serving loop (continuous batching) ----------------------------------
+ * A server owns hbm_budget_bytes of device memory and a persistent device
+ * loop that runs matrix-vector jobs (tk_matvec semantics) from a device-
+ * resident job ring.  tk_server_submit queues a request of njobs jobs of one
+ * k whose buffers are HOST memory (A: njobs*k*k, s/e/out: njobs*k
+ * polynomials; e may be NULL); requests are admitted in arrival order as pool
+ * memory and request slots free up, and their jobs run alongside jobs already
+ * on the GPU.  Results land in out before the ticket completes.  All host
+ * waits take a timeout; the device loop exits after idle_exit_seconds without
+ * work and is relaunched on demand.  While it runs, the device loop occupies
+ * every SM.  No reference counterpart (the reference times fixed batches).
+ * Buffers passed to submit must stay valid until the ticket completes. */
+typedef struct tk_server tk_server;
+typedef struct tk_server_config {
+  size_t hbm_budget_bytes;    /* device pool for admitted requests (0: 1 GiB) */
+  int max_inflight_requests;  /* request slots (0: 1024) */
+  double idle_exit_seconds;   /* device loop idle limit (0: 0.02 s) */
+} tk_server_config;
+int tk_server_create(int device, const tk_server_config *cfg, tk_server **out);
+int tk_server_submit(tk_server *srv, int k, size_t njobs, const int16_t *A, const int16_t *s,
+                     const int16_t *e, int16_t *out, uint64_t *ticket);
+/* TK_SUCCESS once the request completed, TK_ERR_TIMEOUT if it has not. */
+int tk_server_wait(tk_server *srv, uint64_t ticket, double timeout_s);
+/* *done = 1 when complete; *latency_s = submit-to-completion time (or -1). */
+int tk_server_query(tk_server *srv, uint64_t ticket, int *done, double *latency_s);
+/* Forget a completed ticket. */
+int tk_server_release(tk_server *srv, uint64_t ticket);
+int tk_server_stats(tk_server *srv, unsigned long long *jobs_done, unsigned long long *launches);
+/* Waits (up to timeout_s) for outstanding requests, stops the loop, frees all. */
+int tk_server_destroy(tk_server *srv, double timeout_s);
 
 /* ---- process-wide options ---------------------------------------------------
  * TK_OPT_MATVEC_CHUNK_POLYS: vector polynomials per tk_matvec chunk (the
- * chunk's intermediates are meant to stay in L2); 0 restores the default. */
+ * chunk's intermediates are meant to stay in L2); 0 restores the default.
+ * TK_OPT_MATVEC_MODE: TK_MATVEC_PIPELINE (NTT, basemul-accumulate and iNTT+e
+ * as three stream-ordered kernels per chunk) or TK_MATVEC_FUSED (one kernel,
+ * one warp per job: every intermediate stays in shared memory). */
 #define TK_OPT_MATVEC_CHUNK_POLYS 1
+#define TK_OPT_MATVEC_MODE 2
+#define TK_MATVEC_PIPELINE 0
+#define TK_MATVEC_FUSED 1
 int tk_set_option(int option, long long value);
 long long tk_get_option(int option);
 

@@ -27,7 +27,7 @@ CSRC = os.path.join(_HERE, "csrc")
 STATUS = {
     0: "TK_SUCCESS", 1: "TK_ERR_INVALID_VALUE", 2: "TK_ERR_MISALIGNED",
     3: "TK_ERR_TOO_LARGE", 4: "TK_ERR_NO_DEVICE", 5: "TK_ERR_CUDA",
-    6: "TK_ERR_NOT_DEVICE_MEMORY", 7: "TK_ERR_KERNEL_TIMEOUT",
+    6: "TK_ERR_NOT_DEVICE_MEMORY", 7: "TK_ERR_KERNEL_TIMEOUT", 8: "TK_ERR_TIMEOUT",
 }
 
 
@@ -35,6 +35,12 @@ class MatvecBatch(ctypes.Structure):
     """Mirror of tk_matvec_batch (include/tk_ntt.h)."""
     _fields_ = [("k", ctypes.c_int), ("njobs", ctypes.c_size_t), ("A", ctypes.c_void_p),
                 ("s", ctypes.c_void_p), ("e", ctypes.c_void_p), ("out", ctypes.c_void_p)]
+
+
+class ServerConfig(ctypes.Structure):
+    """Mirror of tk_server_config (include/tk_ntt.h)."""
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_inflight_requests", ctypes.c_int),
+                ("idle_exit_seconds", ctypes.c_double)]
 
 
 class TKError(RuntimeError):
@@ -112,6 +118,21 @@ def lib() -> ctypes.CDLL:
     L.tk_autotune_reset.restype = ctypes.c_int
     L.tk_matvec.argtypes = [ctypes.POINTER(MatvecBatch), ctypes.c_int, ctypes.c_void_p]
     L.tk_matvec.restype = ctypes.c_int
+    L.tk_matvec_host.argtypes = [ctypes.POINTER(MatvecBatch), ctypes.c_int]
+    L.tk_matvec_host.restype = ctypes.c_int
+    vp, u64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)
+    L.tk_server_create.argtypes = [ctypes.c_int, ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+    L.tk_server_submit.argtypes = [vp, ctypes.c_int, ctypes.c_size_t, vp, vp, vp, vp, u64p]
+    L.tk_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double]
+    L.tk_server_query.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_double)]
+    L.tk_server_release.argtypes = [vp, ctypes.c_uint64]
+    L.tk_server_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong),
+                                  ctypes.POINTER(ctypes.c_ulonglong)]
+    L.tk_server_destroy.argtypes = [vp, ctypes.c_double]
+    for f in ("tk_server_create", "tk_server_submit", "tk_server_wait", "tk_server_query",
+              "tk_server_release", "tk_server_stats", "tk_server_destroy"):
+        getattr(L, f).restype = ctypes.c_int
     L.tk_set_option.argtypes = [ctypes.c_int, ctypes.c_longlong]
     L.tk_set_option.restype = ctypes.c_int
     L.tk_get_option.argtypes = [ctypes.c_int]
@@ -223,7 +244,81 @@ def matvec(batches, stream=None):
     _check(lib().tk_matvec(arr, len(items), _stream_ptr(stream)))
 
 
+def matvec_host(batches):
+    """tk_matvec on numpy int16 host arrays (synchronous; same shapes as matvec)."""
+    items = []
+    for k, A, s, e, out in batches:
+        n = _host_arr(s) // k
+        if _host_arr(A) != n * k * k or _host_arr(out) != n * k or (
+                e is not None and _host_arr(e) != n * k):
+            raise ValueError("inconsistent matvec batch shapes")
+        items.append(MatvecBatch(k, n, A.ctypes.data, s.ctypes.data,
+                                 e.ctypes.data if e is not None else None, out.ctypes.data))
+    arr = (MatvecBatch * len(items))(*items)
+    _check(lib().tk_matvec_host(arr, len(items)))
+
+
+class Server:
+    """Continuous-batching server for matrix-vector requests (tk_server_*).
+
+    Requests are numpy int16 arrays in host memory: A (njobs, k, k, 256),
+    s / e (njobs, k, 256), out (njobs, k, 256); they must stay alive until the
+    request completes (the object keeps references until release)."""
+
+    def __init__(self, hbm_budget_bytes=1 << 30, max_inflight_requests=1024,
+                 idle_exit_seconds=0.02, device=0):
+        cfg = ServerConfig(hbm_budget_bytes, max_inflight_requests, idle_exit_seconds)
+        h = ctypes.c_void_p()
+        _check(lib().tk_server_create(device, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, k, A, s, e, out) -> int:
+        n = _host_arr(s) // k
+        if _host_arr(A) != n * k * k or _host_arr(out) != n * k or (
+                e is not None and _host_arr(e) != n * k):
+            raise ValueError("inconsistent request shapes")
+        t = ctypes.c_uint64()
+        _check(lib().tk_server_submit(self._h, k, n, A.ctypes.data, s.ctypes.data,
+                                      e.ctypes.data if e is not None else None,
+                                      out.ctypes.data, ctypes.byref(t)))
+        self._keep[t.value] = (A, s, e, out)
+        return t.value
+
+    def wait(self, ticket: int, timeout: float = 30.0) -> None:
+        _check(lib().tk_server_wait(self._h, ticket, timeout))
+
+    def latency(self, ticket: int):
+        done, lat = ctypes.c_int(), ctypes.c_double()
+        _check(lib().tk_server_query(self._h, ticket, ctypes.byref(done), ctypes.byref(lat)))
+        return lat.value if done.value else None
+
+    def release(self, ticket: int) -> None:
+        _check(lib().tk_server_release(self._h, ticket))
+        self._keep.pop(ticket, None)
+
+    def stats(self):
+        jobs, launches = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        _check(lib().tk_server_stats(self._h, ctypes.byref(jobs), ctypes.byref(launches)))
+        return {"jobs_done": jobs.value, "device_loop_launches": launches.value}
+
+    def close(self, timeout: float = 60.0) -> None:
+        if self._h:
+            rc = lib().tk_server_destroy(self._h, timeout)
+            self._h = None
+            self._keep.clear()
+            _check(rc)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 OPT_MATVEC_CHUNK_POLYS = 1
+OPT_MATVEC_MODE = 2
+MATVEC_PIPELINE, MATVEC_FUSED = 0, 1
 
 
 def set_option(option: int, value: int) -> None:

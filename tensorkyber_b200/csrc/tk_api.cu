@@ -7,6 +7,7 @@
 
 #include <atomic>
 #include <mutex>
+#include <vector>
 
 #include "../../include/tk_ntt.h"
 #include "tk_internal.h"
@@ -27,6 +28,11 @@ struct DeviceState {
   int16_t* stage[3] = {nullptr, nullptr, nullptr};
   cudaStream_t streams[3] = {nullptr, nullptr, nullptr};
   size_t stage_polys = 0;
+  // tk_matvec_host staging (grown on demand)
+  std::mutex mv_mu;
+  uint8_t* mv_stage = nullptr;
+  size_t mv_bytes = 0;
+  cudaStream_t mv_stream = nullptr;
 };
 
 DeviceState g_dev[kMaxDevices];
@@ -35,6 +41,7 @@ thread_local char t_err[256] = "";
 // Kernel variant choice: forced by tk_set_variant (>= 0) or picked by size.
 std::atomic<int> g_forced[2] = {{-1}, {-1}};
 std::atomic<long long> g_matvec_chunk{tk::kMatvecChunkVecPolys};
+std::atomic<int> g_matvec_mode{TK_MATVEC_PIPELINE};
 
 const char* const kVariantNames[tk::kNumMmaVariants] = {
     "mma.sync 4 warps x 32-poly tiles, 3-slot TMA ring",
@@ -259,6 +266,13 @@ int run_host(bool inverse, int16_t* polys, size_t npoly) {
 
 }  // namespace
 
+namespace tk {
+int api_device_info(int device, DeviceInfo** info) {
+  if (device < 0 || device >= kMaxDevices) return TK_ERR_INVALID_VALUE;
+  return ensure_ready(device, info);
+}
+}  // namespace tk
+
 extern "C" {
 
 int tk_ntt(int16_t* polys, size_t npoly, tk_stream_t stream) {
@@ -280,8 +294,11 @@ static bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
   return x < y + nb && y < x + na;
 }
 
-int tk_matvec(const tk_matvec_batch* batches, int nbatches, tk_stream_t stream) {
-  t_err[0] = 0;
+// Checks of a batch list common to the device and host forms; *nonempty =
+// batches with work.  host: pointers are host memory (no alignment or overlap
+// rule, the data is staged).
+static int validate_matvec(const tk_matvec_batch* batches, int nbatches, bool host,
+                           int* nonempty_out) {
   if (nbatches < 0 || (nbatches > 0 && !batches)) {
     set_msg("tk_matvec: bad batch list");
     return TK_ERR_INVALID_VALUE;
@@ -303,6 +320,7 @@ int tk_matvec(const tk_matvec_batch* batches, int nbatches, tk_stream_t stream) 
       set_msg("tk_matvec: too many jobs in one batch");
       return TK_ERR_TOO_LARGE;
     }
+    if (host) continue;
     if ((((uintptr_t)B.A | (uintptr_t)B.s | (uintptr_t)B.e | (uintptr_t)B.out) & 15u) != 0) {
       set_msg("tk_matvec: buffers must be 16-byte aligned");
       return TK_ERR_MISALIGNED;
@@ -314,19 +332,39 @@ int tk_matvec(const tk_matvec_batch* batches, int nbatches, tk_stream_t stream) 
       return TK_ERR_INVALID_VALUE;
     }
   }
-  if (nonempty == 0) return TK_SUCCESS;
-  int dev;
-  int rc = current_device(&dev);
-  if (rc) return rc;
-  DeviceInfo* info;
-  rc = ensure_ready(dev, &info);
-  if (rc) return rc;
-  for (int b = 0; b < nbatches; b++) {
-    const tk_matvec_batch& B = batches[b];
-    if (B.njobs == 0) continue;
-    const void* ptrs[4] = {B.A, B.s, B.out, B.e};
-    for (const void* p : ptrs)
-      if (p && (rc = check_device_ptr(p))) return rc;
+  *nonempty_out = nonempty;
+  return TK_SUCCESS;
+}
+
+// Launches a validated batch list of device buffers.
+static int launch_matvec_batches(const tk_matvec_batch* batches, int nbatches,
+                                 const DeviceInfo* info, cudaStream_t stream) {
+  if (g_matvec_mode.load(std::memory_order_relaxed) == TK_MATVEC_FUSED) {
+    // single-launch fused kernel, up to three batches per launch
+    tk::FusedBatches fb{};
+    int b = 0;
+    while (b < nbatches) {
+      fb.nb = 0;
+      fb.first[0] = 0;
+      for (; b < nbatches && fb.nb < 3; b++) {
+        const tk_matvec_batch& B = batches[b];
+        if (B.njobs == 0) continue;
+        fb.k[fb.nb] = B.k;
+        fb.A[fb.nb] = B.A;
+        fb.s[fb.nb] = B.s;
+        fb.e[fb.nb] = B.e;
+        fb.out[fb.nb] = B.out;
+        fb.first[fb.nb + 1] = fb.first[fb.nb] + (int)B.njobs;
+        fb.nb++;
+      }
+      if (fb.nb == 0) break;
+      cudaError_t e = tk::launch_matvec_fused(fb, *info, (cudaStream_t)stream);
+      if (e != cudaSuccess) {
+        set_launch_err(e);
+        return TK_ERR_CUDA;
+      }
+    }
+    return TK_SUCCESS;
   }
   for (int b = 0; b < nbatches; b++) {
     const tk_matvec_batch& B = batches[b];
@@ -342,6 +380,106 @@ int tk_matvec(const tk_matvec_batch* batches, int nbatches, tk_stream_t stream) 
   }
   return TK_SUCCESS;
 }
+
+int tk_matvec(const tk_matvec_batch* batches, int nbatches, tk_stream_t stream) {
+  t_err[0] = 0;
+  int nonempty = 0;
+  int rc = validate_matvec(batches, nbatches, false, &nonempty);
+  if (rc || nonempty == 0) return rc;
+  int dev;
+  if ((rc = current_device(&dev))) return rc;
+  DeviceInfo* info;
+  if ((rc = ensure_ready(dev, &info))) return rc;
+  for (int b = 0; b < nbatches; b++) {
+    const tk_matvec_batch& B = batches[b];
+    if (B.njobs == 0) continue;
+    const void* ptrs[4] = {B.A, B.s, B.out, B.e};
+    for (const void* p : ptrs)
+      if (p && (rc = check_device_ptr(p))) return rc;
+  }
+  return launch_matvec_batches(batches, nbatches, info, (cudaStream_t)stream);
+}
+
+int tk_matvec_host(const tk_matvec_batch* batches, int nbatches) {
+  t_err[0] = 0;
+  int nonempty = 0;
+  int rc = validate_matvec(batches, nbatches, true, &nonempty);
+  if (rc || nonempty == 0) return rc;
+  constexpr size_t kAlign = 256, kMaxStage = (size_t)8 << 30;
+  auto up = [](size_t n) { return (n + kAlign - 1) & ~(kAlign - 1); };
+  size_t need = 0;
+  for (int b = 0; b < nbatches; b++) {
+    const tk_matvec_batch& B = batches[b];
+    const size_t vb = B.njobs * (size_t)B.k * 512u;
+    need += up(vb * (size_t)B.k) + up(vb) * (B.e ? 3 : 2);
+  }
+  if (need > kMaxStage) {
+    set_msg("tk_matvec_host: batch list above the 8 GiB staging limit");
+    return TK_ERR_TOO_LARGE;
+  }
+  int dev;
+  if ((rc = current_device(&dev))) return rc;
+  DeviceInfo* info;
+  if ((rc = ensure_ready(dev, &info))) return rc;
+  DeviceState& S = g_dev[dev];
+  std::lock_guard<std::mutex> lk(S.mv_mu);
+  cudaError_t e = cudaSuccess;
+  if (!S.mv_stream) e = cudaStreamCreateWithFlags(&S.mv_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess && S.mv_bytes < need) {
+    if (S.mv_stage) cudaFree(S.mv_stage);
+    S.mv_stage = nullptr;
+    S.mv_bytes = 0;
+    e = cudaMalloc(&S.mv_stage, need);
+    if (e == cudaSuccess) S.mv_bytes = need;
+  }
+  if (e != cudaSuccess) {
+    set_err("tk_matvec_host staging", e);
+    return e == cudaErrorMemoryAllocation ? TK_ERR_TOO_LARGE : TK_ERR_CUDA;
+  }
+  std::vector<tk_matvec_batch> dev_batches((size_t)nbatches);
+  cudaStream_t st = S.mv_stream;
+  size_t off = 0;
+  for (int b = 0; b < nbatches && e == cudaSuccess; b++) {
+    const tk_matvec_batch& B = batches[b];
+    tk_matvec_batch& D = dev_batches[(size_t)b];
+    D = B;
+    if (B.njobs == 0) continue;
+    const size_t vb = B.njobs * (size_t)B.k * 512u, ab = vb * (size_t)B.k;
+    int16_t* dA = (int16_t*)(S.mv_stage + off);
+    int16_t* ds = (int16_t*)(S.mv_stage + off + up(ab));
+    int16_t* dout = (int16_t*)(S.mv_stage + off + up(ab) + up(vb));
+    int16_t* de = B.e ? (int16_t*)(S.mv_stage + off + up(ab) + 2 * up(vb)) : nullptr;
+    off += up(ab) + up(vb) * (B.e ? 3 : 2);
+    e = cudaMemcpyAsync(dA, B.A, ab, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ds, B.s, vb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && de) e = cudaMemcpyAsync(de, B.e, vb, cudaMemcpyHostToDevice, st);
+    D.A = dA;
+    D.s = ds;
+    D.e = de;
+    D.out = dout;
+  }
+  if (e == cudaSuccess) {
+    rc = launch_matvec_batches(dev_batches.data(), nbatches, info, st);
+    if (rc) {
+      cudaStreamSynchronize(st);
+      return rc;
+    }
+  }
+  for (int b = 0; b < nbatches && e == cudaSuccess; b++) {
+    const tk_matvec_batch& B = batches[b];
+    if (B.njobs == 0) continue;
+    e = cudaMemcpyAsync(B.out, dev_batches[(size_t)b].out, B.njobs * (size_t)B.k * 512u,
+                        cudaMemcpyDeviceToHost, st);
+  }
+  const cudaError_t e2 = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = e2;
+  if (e != cudaSuccess) {
+    set_err("tk_matvec_host", e);
+    return TK_ERR_CUDA;
+  }
+  return TK_SUCCESS;
+}
+
 int tk_invntt_host(int16_t* polys, size_t npoly) { return run_host(true, polys, npoly); }
 
 int tk_init(int device) {
@@ -399,6 +537,7 @@ const char* tk_status_string(int status) {
     case TK_ERR_CUDA: return "CUDA runtime error";
     case TK_ERR_NOT_DEVICE_MEMORY: return "pointer is not device memory";
     case TK_ERR_KERNEL_TIMEOUT: return "kernel bounded wait timed out";
+    case TK_ERR_TIMEOUT: return "host wait timed out";
     default: return "unknown status";
   }
 }
@@ -430,6 +569,10 @@ int tk_set_option(int option, long long value) {
       if (value < 0 || value > (1ll << 30)) break;
       g_matvec_chunk.store(value == 0 ? tk::kMatvecChunkVecPolys : value);
       return TK_SUCCESS;
+    case TK_OPT_MATVEC_MODE:
+      if (value != TK_MATVEC_PIPELINE && value != TK_MATVEC_FUSED) break;
+      g_matvec_mode.store((int)value);
+      return TK_SUCCESS;
     default:
       break;
   }
@@ -440,6 +583,7 @@ int tk_set_option(int option, long long value) {
 long long tk_get_option(int option) {
   switch (option) {
     case TK_OPT_MATVEC_CHUNK_POLYS: return g_matvec_chunk.load();
+    case TK_OPT_MATVEC_MODE: return g_matvec_mode.load();
     default: return -TK_ERR_INVALID_VALUE;
   }
 }

@@ -41,10 +41,56 @@ int last_encode_result();
 // polynomials, so that intermediates stay in the 126 MB L2.
 constexpr long long kMatvecChunkVecPolys = 131072;  // default (64 MiB); tk_set_option may change it
 bool matvec_init_device();
+// Up to three uniform-k batches for the single-launch fused kernel: global job
+// g belongs to batch b when first[b] <= g < first[b+1].
+struct FusedBatches {
+  int nb;
+  int k[3];
+  int first[4];
+  const int16_t* A[3];
+  const int16_t* s[3];
+  const int16_t* e[3];
+  int16_t* out[3];
+};
+cudaError_t launch_matvec_fused(const FusedBatches& args, const DeviceInfo& info,
+                                cudaStream_t stream);
 cudaError_t launch_matvec(int k, size_t njobs, const int16_t* A, const int16_t* s,
                           const int16_t* e, int16_t* out, const DeviceInfo& info,
                           cudaStream_t stream, int fwd_variant, int inv_variant,
                           long long chunk_vec_polys);
+
+// ---- serving loop (device side in tk_matvec.cu, host side in tk_serve.cpp) ----
+// One job descriptor of the device-resident ring (64 bytes).
+struct ServeJob {
+  const int16_t* A;
+  const int16_t* s;
+  const int16_t* e;
+  int16_t* out;
+  uint32_t k;
+  uint32_t req;    // request slot
+  uint32_t njobs;  // jobs of the request
+  uint32_t gen;    // request generation written to the completion flag
+  uint64_t pad[2];
+};
+// Device-memory control block.  head: jobs claimed (device atomics); tail:
+// jobs published (written by the host with stream-ordered copy-engine
+// memsets); both count modulo 2^32 and are compared as (int)(tail - head);
+// stop: set by the host to end the loop.
+struct ServeCtl {
+  unsigned int head;
+  unsigned int tail;
+  unsigned int stop;
+  unsigned int pad;
+};
+// Launches the persistent serving kernel.  req_ctr: per-slot done counters
+// (device memory); req_flag: per-slot completion flags in mapped pinned host
+// memory; idle_ns: the loop exits after this long without a claimable job.
+cudaError_t launch_serve(const ServeJob* ring, uint32_t ring_mask, ServeCtl* ctl,
+                         unsigned int* req_ctr, unsigned int* req_flag, unsigned long long idle_ns,
+                         const DeviceInfo& info, cudaStream_t stream);
+
+// Per-device state of the API layer (set-up on first use), for other units.
+int api_device_info(int device, DeviceInfo** info);
 
 // Kernel-side error flags (bounded waits that gave up), read and reset.
 cudaError_t read_and_clear_status(unsigned* flags);

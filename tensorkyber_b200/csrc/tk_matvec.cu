@@ -23,6 +23,8 @@
 
 #include "tk_internal.h"
 #include "tk_ptx.cuh"
+#include "tk_stages.cuh"
+#include "tk_tables.h"
 
 namespace tk {
 
@@ -109,7 +111,370 @@ static bool upload_pair_constants() {
   return cudaMemcpyToSymbol(g_bm_zr, zr, sizeof(zr)) == cudaSuccess;
 }
 
-bool matvec_init_device() { return upload_pair_constants(); }
+// ============================================================================
+// Fused single-launch form: one warp runs a whole job, forward NTT of s,
+// basemul-accumulate, inverse NTT plus e, in an 8-row padded smem buffer (rows
+// >= k hold stale data; their results are never stored).  The per-block
+// constants of both block-wise stages sit in CTA-shared smem, the stage-over-m
+// constants and the pair constants in registers.  Used for the single-launch
+// matvec mode and by the serving loop (tk_serve.cu).
+// ============================================================================
+__device__ FwdFrags g_mv_fwd;
+__device__ InvFrags g_mv_inv;
+
+// smem constants, per block pair P (blocks 2P, 2P+1) and lane: 8 words of
+// fragments (block 2P even, 2P odd, 2P+1 even, 2P+1 odd; 2 words each), and
+// for the inverse 4 accumulator-init words.
+struct FusedConsts {
+  uint32_t fwd[8][32][8];
+  uint32_t inv[8][32][8];
+  int32_t inv_c[8][32][4];
+};
+constexpr int kFusedConstBytes = (int)sizeof(FusedConsts);
+
+__device__ __forceinline__ void fused_load_consts(FusedConsts* C) {
+  for (int idx = threadIdx.x; idx < 8 * 32; idx += blockDim.x) {
+    const int P = idx >> 5, lane = idx & 31;
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int sp = 0; sp < 2; sp++) {
+        const int b = 2 * P + h;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+          C->fwd[P][lane][4 * h + 2 * sp + j] = g_mv_fwd.s2[b][sp][lane][j];
+          C->inv[P][lane][4 * h + 2 * sp + j] = g_mv_inv.sa[b][sp][lane][j];
+        }
+        C->inv_c[P][lane][2 * h + sp] = g_mv_inv.ca[b][sp][lane];
+      }
+  }
+}
+
+struct WarpRegs {
+  uint32_t am_f[2][4], am_i[2][4];
+  int32_t c1lo, c1hi;
+  uint32_t zr[4];
+};
+
+// Global loads of a job's inputs.  kL2Only (the serving loop, whose memory
+// pool is reused by later requests) reads at L2 only, so an L1 line left from
+// an earlier request can never be returned.
+template <bool kL2Only>
+__device__ __forceinline__ uint4 job_ld16(const void* p) {
+  return kL2Only ? __ldcg((const uint4*)p) : __ldcs((const uint4*)p);
+}
+template <bool kL2Only>
+__device__ __forceinline__ uint32_t job_ld4(const void* p) {
+  return kL2Only ? __ldcg((const uint32_t*)p) : __ldcs((const uint32_t*)p);
+}
+
+// One job of width k (2..4) on this warp.  rows/rowp: the warp's 8 x 528-byte
+// buffer (smem address / pointer).
+template <bool kL2Only>
+__device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
+                                          const int16_t* __restrict__ s,
+                                          const int16_t* __restrict__ e, int16_t* __restrict__ out,
+                                          uint32_t rows, uint8_t* rowp, const FusedConsts* C,
+                                          const WarpRegs& R, int lane) {
+  const int q4 = lane & 3, g8 = lane >> 2;
+  const uint32_t ldt_off = 32u * ((lane & 7) + 8 * ((lane >> 3) & 1)) + 16u * (lane >> 4);
+  const uint32_t hb1 = (lane >> 4) & 1;
+  const uint32_t w_even = 32u * g8 + 16u * hb1 + 4u * q4;
+  const uint32_t w_odd = 32u * g8 + 16u * (hb1 ^ 1) + 4u * q4;
+  const uint32_t w_nat = 32u * g8 + 4u * q4;
+  const uint32_t row_l = kRowBytes * (lane & 7) + 32u * (lane >> 4);
+  const uint32_t stc_off = kRowBytes * (2 * q4) + 4u * g8;
+  const uint32_t zero_add[4] = {0, 0, 0, 0};
+
+  // 1. s -> rows (each lane moves 16 bytes of every polynomial)
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    if (j < k) {
+      const uint4 v = job_ld16<kL2Only>(s + j * 256 + 8 * lane);
+      *(uint4*)(rowp + j * kRowBytes + 16 * lane) = v;
+    }
+  __syncwarp();
+  // 2. forward stage 1 (M1), x ^ 0x8000 bias, parity-split rows
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    if (j < k) {
+      uint32_t b[4];
+      ldsm_x4_t(rows + j * kRowBytes + ldt_off, b[0], b[1], b[2], b[3]);
+      stage_m<false>(R.am_f, R.c1lo, R.c1hi, b[0] ^ 0x80008000u, b[1] ^ 0x80008000u,
+                     b[2] ^ 0x80008000u, b[3] ^ 0x80008000u, rowp + j * kRowBytes, w_even, w_odd,
+                     0, zero_add);
+    }
+  __syncwarp();
+  // 3. forward stage 2 (M2), all 8 block pairs on the 8-row n-tile
+#pragma unroll 2
+  for (int P = 0; P < 8; P++) {
+    const uint32_t hbw = (P >> 1) & 1;
+    uint32_t r[4];
+    ldsm_x4(rows + 64u * P + row_l + 16u * (((lane >> 3) & 1) ^ hbw), r[0], r[1], r[2], r[3]);
+    const uint4 f0 = *(const uint4*)&C->fwd[P][lane][0];
+    const uint4 f1 = *(const uint4*)&C->fwd[P][lane][4];
+    const uint32_t a[2][2][2] = {{{f0.x, f0.y}, {f0.z, f0.w}}, {{f1.x, f1.y}, {f1.z, f1.w}}};
+    const int32_t zc[2][2] = {{0, 0}, {0, 0}};
+    stage_c<false>(a, zc, r, rowp + 64 * P + stc_off);
+  }
+  __syncwarp();
+  // 4. basemul-accumulate over j, accumulators in registers; acc_i -> row i
+  int32_t acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int u = 0; u < 4; u++) acc[i][u][0] = acc[i][u][1] = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    if (j < k) {
+      const uint4 v = *(const uint4*)(rowp + j * kRowBytes + 16 * lane);
+      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+      uint32_t B0[4], B1[4], Bz[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        B0[u] = mulmod_lazy(w[u] & 0xffffu, kRinv);
+        B1[u] = mulmod_lazy(w[u] >> 16, kRinv);
+        Bz[u] = mulmod_lazy(w[u] >> 16, R.zr[u]);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        if (i < k) {
+          const uint4 av = job_ld16<kL2Only>(A + (i * k + j) * 256 + 8 * lane);
+          const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const int32_t a0 = (int16_t)(aw[u] & 0xffffu), a1 = (int32_t)aw[u] >> 16;
+            acc[i][u][0] += a0 * (int32_t)B0[u] + a1 * (int32_t)Bz[u];
+            acc[i][u][1] += a0 * (int32_t)B1[u] + a1 * (int32_t)B0[u];
+          }
+        }
+    }
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+    if (i < k) {
+      uint32_t o[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        o[u] = pack2(red_wide((uint32_t)acc[i][u][0] + kAccBias),
+                     red_wide((uint32_t)acc[i][u][1] + kAccBias));
+      *(uint4*)(rowp + i * kRowBytes + 16 * lane) = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+  __syncwarp();
+  // 5. inverse stage A (MA), natural order in and out
+#pragma unroll 2
+  for (int P = 0; P < 8; P++) {
+    uint32_t r[4];
+    ldsm_x4(rows + 64u * P + row_l + 16u * ((lane >> 3) & 1), r[0], r[1], r[2], r[3]);
+    const uint32_t x0 = r[0] ^ 0x80008000u, x1 = r[1] ^ 0x80008000u;
+    const uint32_t x2 = r[2] ^ 0x80008000u, x3 = r[3] ^ 0x80008000u;
+    const uint32_t x[4] = {__byte_perm(x0, x1, 0x5410), __byte_perm(x0, x1, 0x7632),
+                           __byte_perm(x2, x3, 0x5410), __byte_perm(x2, x3, 0x7632)};
+    const uint4 f0 = *(const uint4*)&C->inv[P][lane][0];
+    const uint4 f1 = *(const uint4*)&C->inv[P][lane][4];
+    const int4 cv = *(const int4*)&C->inv_c[P][lane][0];
+    const uint32_t a[2][2][2] = {{{f0.x, f0.y}, {f0.z, f0.w}}, {{f1.x, f1.y}, {f1.z, f1.w}}};
+    const int32_t ca[2][2] = {{cv.x, cv.y}, {cv.z, cv.w}};
+    stage_c<true>(a, ca, x, rowp + 64 * P + stc_off);
+  }
+  __syncwarp();
+  // 6. inverse stage B (Minv), centred, plus e
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    if (j < k) {
+      uint32_t add[4] = {0, 0, 0, 0};
+      if (e) {
+        const uint32_t* ew = (const uint32_t*)(e + j * 256) + 8 * g8 + q4;
+        add[0] = job_ld4<kL2Only>(ew);
+        add[1] = job_ld4<kL2Only>(ew + 4);
+        add[2] = job_ld4<kL2Only>(ew + 64);
+        add[3] = job_ld4<kL2Only>(ew + 68);
+      }
+      uint32_t b[4];
+      ldsm_x4_t(rows + j * kRowBytes + ldt_off, b[0], b[1], b[2], b[3]);
+      stage_m<true>(R.am_i, 1664, 1664, b[0], b[1], b[2], b[3], rowp + j * kRowBytes, 0, 0, w_nat,
+                    add);
+    }
+  __syncwarp();
+  // 7. rows -> out
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    if (j < k) {
+      const uint4 v = *(const uint4*)(rowp + j * kRowBytes + 16 * lane);
+      __stcs((uint4*)(out + j * 256 + 8 * lane), v);
+    }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void fused_warp_regs(WarpRegs& R, int lane) {
+#pragma unroll
+  for (int g = 0; g < 2; g++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      R.am_f[g][j] = g_mv_fwd.s1[g][lane][j];
+      R.am_i[g][j] = g_mv_inv.sb[g][lane][j];
+    }
+  R.c1lo = g_mv_fwd.c1[lane][0];
+  R.c1hi = g_mv_fwd.c1[lane][1];
+#pragma unroll
+  for (int u = 0; u < 4; u++) R.zr[u] = (uint32_t)g_bm_zr[4 * lane + u];
+}
+
+constexpr int kFusedWarps = 4;
+constexpr int kFusedWarpBytes = 8 * kRowBytes;
+constexpr int kFusedSmem = kFusedConstBytes + kFusedWarps * kFusedWarpBytes;
+
+__global__ void __launch_bounds__(32 * kFusedWarps)
+    k_matvec_fused(const __grid_constant__ FusedBatches args) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  FusedConsts* C = (FusedConsts*)smem;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint8_t* rowp = smem + kFusedConstBytes + warp * kFusedWarpBytes;
+  const uint32_t rows = smem_u32(rowp);
+  fused_load_consts(C);
+  WarpRegs R;
+  fused_warp_regs(R, lane);
+  __syncthreads();
+  grid_dependency_wait();
+  grid_launch_dependents();
+  const int total = args.first[args.nb];
+  const int gw = blockIdx.x * kFusedWarps + warp, nw = gridDim.x * kFusedWarps;
+  for (int job = gw; job < total; job += nw) {
+    int b = 0;
+    while (b + 1 < args.nb && job >= args.first[b + 1]) b++;
+    const int k = args.k[b];
+    const size_t t = (size_t)(job - args.first[b]);
+    fused_job<false>(k, args.A[b] + t * k * k * 256, args.s[b] + t * k * 256,
+              args.e[b] ? args.e[b] + t * k * 256 : nullptr, args.out[b] + t * k * 256, rows, rowp,
+              C, R, lane);
+  }
+}
+
+// ============================================================================
+// Serving loop: a persistent kernel whose warps claim published jobs from the
+// device-resident ring (compare-and-swap on head only while head < tail, so an
+// unpublished slot is never claimed and the loop may exit at any idle point),
+// run fused_job on them, and count completions per request; the warp that
+// completes a request fences its outputs system-wide and writes the request's
+// generation into the request's flag in mapped host memory.  Every wait is
+// bounded: a warp leaves the loop after idle_ns without a claimable job, or
+// as soon as the host sets ctl->stop.
+// ============================================================================
+__global__ void __launch_bounds__(32 * kFusedWarps)
+    k_serve(const ServeJob* __restrict__ ring, uint32_t ring_mask, ServeCtl* ctl,
+            unsigned int* req_ctr, unsigned int* req_flag, unsigned long long idle_ns) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  FusedConsts* C = (FusedConsts*)smem;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint8_t* rowp = smem + kFusedConstBytes + warp * kFusedWarpBytes;
+  const uint32_t rows = smem_u32(rowp);
+  fused_load_consts(C);
+  WarpRegs R;
+  fused_warp_regs(R, lane);
+  __syncthreads();
+  volatile unsigned int* stop = &ctl->stop;
+  while (true) {
+    unsigned long long got = ~0ull;
+    if (lane == 0) {
+      unsigned long long t0 = globaltimer_ns();
+      while (true) {
+        unsigned int h, t;
+        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(h) : "l"(&ctl->head) : "memory");
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(t) : "l"(&ctl->tail) : "memory");
+        if ((int)(t - h) > 0) {
+          if (atomicCAS(&ctl->head, h, h + 1) == h) {
+            got = h;
+            break;
+          }
+          continue;
+        }
+        if (*stop) break;
+        if (globaltimer_ns() - t0 > idle_ns) break;
+        __nanosleep(500);
+      }
+    }
+    got = __shfl_sync(0xffffffffu, got, 0);
+    if (got == ~0ull) break;  // warp-uniform exit
+    const ServeJob* J = ring + (got & ring_mask);
+    const int16_t* A = (const int16_t*)__ldcg((const unsigned long long*)&J->A);
+    const int16_t* sv = (const int16_t*)__ldcg((const unsigned long long*)&J->s);
+    const int16_t* ev = (const int16_t*)__ldcg((const unsigned long long*)&J->e);
+    int16_t* out = (int16_t*)__ldcg((const unsigned long long*)&J->out);
+    const uint4 meta = __ldcg((const uint4*)&J->k);  // k, req, njobs, gen
+    fused_job<true>((int)meta.x, A, sv, ev, out, rows, rowp, C, R, lane);
+    if (lane == 0) {
+      __threadfence();
+      const unsigned int done = atomicAdd(&req_ctr[meta.y], 1u) + 1u;
+      if (done == meta.z) {
+        // every job of the request has counted: reset the counter for the
+        // slot's next request (admitted only after the host sees the flag)
+        req_ctr[meta.y] = 0u;
+        __threadfence_system();
+        asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(&req_flag[meta.y]), "r"(meta.w)
+                     : "memory");
+      }
+    }
+    __syncwarp();
+  }
+}
+
+cudaError_t launch_serve(const ServeJob* ring, uint32_t ring_mask, ServeCtl* ctl,
+                         unsigned int* req_ctr, unsigned int* req_flag, unsigned long long idle_ns,
+                         const DeviceInfo& info, cudaStream_t stream) {
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [] {
+    attr_err = cudaFuncSetAttribute(k_serve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kFusedSmem);
+  });
+  if (attr_err != cudaSuccess) return attr_err;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_serve, 32 * kFusedWarps, kFusedSmem);
+  const unsigned blocks = (unsigned)(info.num_sms * (per_sm > 0 ? per_sm : 1));
+  k_serve<<<blocks, 32 * kFusedWarps, kFusedSmem, stream>>>(ring, ring_mask, ctl, req_ctr, req_flag,
+                                                           idle_ns);
+  return cudaGetLastError();
+}
+
+static bool upload_fused_tables() {
+  static Matrices M;
+  static FwdFrags FF;
+  static InvFrags IF;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    build_matrices(&M);
+    build_fwd_frags(M, &FF);
+    build_inv_frags(M, &IF);
+  });
+  return cudaMemcpyToSymbol(g_mv_fwd, &FF, sizeof(FF)) == cudaSuccess &&
+         cudaMemcpyToSymbol(g_mv_inv, &IF, sizeof(IF)) == cudaSuccess &&
+         cudaFuncSetAttribute(k_matvec_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kFusedSmem) == cudaSuccess;
+}
+
+cudaError_t launch_matvec_fused(const FusedBatches& args, const DeviceInfo& info,
+                                cudaStream_t stream) {
+  const int total = args.first[args.nb];
+  if (total <= 0) return cudaSuccess;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_matvec_fused, 32 * kFusedWarps,
+                                                kFusedSmem);
+  long long blocks = (total + kFusedWarps - 1) / kFusedWarps;
+  const long long cap = (long long)info.num_sms * (per_sm > 0 ? per_sm : 1);
+  if (blocks > cap) blocks = cap;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)blocks);
+  cfg.blockDim = dim3(32 * kFusedWarps);
+  cfg.dynamicSmemBytes = kFusedSmem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_matvec_fused, args);
+}
+
+bool matvec_init_device() { return upload_pair_constants() && upload_fused_tables(); }
 
 template <int K>
 static cudaError_t launch_basemul(const int16_t* A, int16_t* vec, int njobs, const DeviceInfo& info,

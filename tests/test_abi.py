@@ -46,7 +46,7 @@ def test_every_declared_symbol_is_exported(tk):
 def test_abi_version_and_strings(tk):
     L = tk.lib()
     assert L.tk_abi_version() == 1
-    for code in range(8):
+    for code in range(9):
         assert L.tk_status_string(code)
     assert L.tk_status_string(99) == b"unknown status"
     assert tk.variant_count() >= 1
@@ -108,3 +108,29 @@ def test_matvec_argument_errors_without_gpu(tk):
     assert L.tk_matvec(arr, 1, None) == 1
     arr = (B * 1)(B(2, 0, None, None, None, None))                  # empty batch: no-op
     assert L.tk_matvec(arr, 1, None) == 0
+
+
+def test_server_argument_errors_without_gpu(tk):
+    import ctypes
+    L = tk.lib()
+    h = ctypes.c_void_p()
+    assert L.tk_server_create(0, None, None) == 1
+    bad = tk.ServerConfig(100, 0, 0.0)                 # budget below 4 KiB
+    assert L.tk_server_create(0, ctypes.byref(bad), ctypes.byref(h)) == 1
+    t = ctypes.c_uint64()
+    assert L.tk_server_submit(None, 2, 1, None, None, None, None, ctypes.byref(t)) == 1
+    assert L.tk_server_wait(None, 1, 0.0) == 1
+    assert L.tk_server_destroy(None, 0.0) == 1
+
+
+def test_matvec_host_argument_errors_without_gpu(tk):
+    L = tk.lib()
+    B = tk.MatvecBatch
+    assert L.tk_matvec_host(None, 0) == 0
+    assert L.tk_matvec_host(None, 1) == 1
+    buf = np.zeros(64 * 256, dtype=np.int16)
+    p = buf.ctypes.data
+    assert L.tk_matvec_host((B * 1)(B(5, 1, p, p, None, p)), 1) == 1
+    assert L.tk_matvec_host((B * 1)(B(2, 1, None, p, None, p)), 1) == 1
+    assert L.tk_matvec_host((B * 1)(B(2, 1 << 29, p, p, None, p)), 1) == 3
+    assert L.tk_matvec_host((B * 1)(B(4, 1 << 27, p, p, p, p)), 1) == 3   # > 8 GiB staging

@@ -10,6 +10,13 @@ from py_oracle import Q, canon
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(params=[0, 1], ids=["pipeline", "fused"])
+def mode(request, tk):
+    tk.set_option(tk.OPT_MATVEC_MODE, request.param)
+    yield request.param
+    tk.set_option(tk.OPT_MATVEC_MODE, 0)
+
+
 def make_jobs(seed, k, n, a_lo=0, a_hi=Q, small=3):
     r = rng(seed)
     A = r.integers(a_lo, a_hi, size=(n, k, k, 256)).astype(np.int16)
@@ -37,20 +44,20 @@ def run(tk, cuda, items, inplace=False):
 
 
 @pytest.mark.parametrize("k", [2, 3, 4])
-def test_matvec_each_k(tk, cuda, oracle, k):
+def test_matvec_each_k(tk, cuda, oracle, mode, k):
     A, s, e = make_jobs(k, k, 203)
     (out,) = run(tk, cuda, [(k, A, s, e)])
     assert (canon(out) == canon(oracle_out(oracle, k, A, s, e))).all()
 
 
-def test_matvec_mixed_batches_one_call(tk, cuda, oracle):
+def test_matvec_mixed_batches_one_call(tk, cuda, oracle, mode):
     items = [(k,) + make_jobs(10 + k, k, n) for k, n in ((3, 77), (2, 130), (4, 51))]
     outs = run(tk, cuda, items)
     for (k, A, s, e), out in zip(items, outs):
         assert (canon(out) == canon(oracle_out(oracle, k, A, s, e))).all()
 
 
-def test_matvec_no_addend_in_place_and_wide_inputs(tk, cuda, oracle):
+def test_matvec_no_addend_in_place_and_wide_inputs(tk, cuda, oracle, mode):
     """e = NULL, out == s, A over (-q, q) and s over the full int16 range."""
     k = 3
     A, s, _ = make_jobs(21, k, 64, a_lo=-Q + 1, a_hi=Q)
@@ -61,11 +68,15 @@ def test_matvec_no_addend_in_place_and_wide_inputs(tk, cuda, oracle):
     assert (canon(out) == canon(ref)).all()
 
 
-def test_matvec_spans_several_chunks(tk, cuda, oracle):
-    """k = 2 with more jobs than one L2-sized chunk (16384 jobs for k = 2)."""
+def test_matvec_spans_several_chunks(tk, cuda, oracle, mode):
+    """k = 2 with more jobs than one chunk (chunk set to 32768 vector polys)."""
     k, n = 2, 40000
     A, s, e = make_jobs(31, k, n)
-    (out,) = run(tk, cuda, [(k, A, s, e)])
+    tk.set_option(tk.OPT_MATVEC_CHUNK_POLYS, 32768)
+    try:
+        (out,) = run(tk, cuda, [(k, A, s, e)])
+    finally:
+        tk.set_option(tk.OPT_MATVEC_CHUNK_POLYS, 0)
     pick = np.r_[0:50, 16380:16390, n - 50:n]
     assert (canon(out[pick]) == canon(oracle_out(oracle, k, A[pick], s[pick], e[pick]))).all()
     assert tk.device_status(0) == 0
@@ -85,3 +96,23 @@ def test_matvec_rejects_bad_batches(tk, cuda):
     assert L.tk_matvec(None, 0, None) == 0
     assert L.tk_matvec(None, 1, None) == 1
     del ctypes
+
+
+def test_matvec_host_matches_device(tk, cuda, oracle, mode):
+    """The host-buffer form (staging + the same kernels) on a mixed list."""
+    r = rng(77)
+    items, expect = [], []
+    for k, n in ((2, 3), (4, 2), (3, 5)):
+        A = r.integers(0, 3329, size=(n, k, k, 256)).astype(np.int16)
+        s = r.integers(-3, 4, size=(n, k, 256)).astype(np.int16)
+        e = r.integers(-3, 4, size=(n, k, 256)).astype(np.int16)
+        out = np.zeros_like(s)
+        items.append((k, A, s, e, out))
+        expect.append(np.stack([oracle.matvec_job(k, A[t].reshape(k * k, 256), s[t], e[t])
+                                for t in range(n)]))
+    tk.matvec_host(items)
+    for (k, A, s, e, out), x in zip(items, expect):
+        assert (canon(out) == canon(x)).all()
+    k, A, s, e, out = items[2]
+    tk.matvec_host([(k, A, s, None, s)])                 # in place, no addend
+    assert (canon(s) == canon(expect[2] - e)).all()
