@@ -62,6 +62,7 @@ def parse():
     p.add_argument("--serve-rates", default="0.25,0.5,0.9,1.5,3,6",
                    help="offered load as multiples of the plain per-request capacity")
     p.add_argument("--serve-templates", type=int, default=256)
+    p.add_argument("--serve-zero-copy", action="store_true")
     return p.parse_args()
 
 
@@ -480,12 +481,15 @@ def run_serve(args):
     """Serving loop against the plain per-request launch, on the same requests.
 
     A request is njobs ~ U{1..64} matrix-vector jobs of one k ~ U{2,3,4} with
-    every coefficient uniform in [0, q) (seeded), in pinned host memory.
+    every coefficient uniform in [0, q) (seeded), in pinned host memory, its
+    A, s and e back to back in one buffer (one copy in, for both arms).
     Arrivals are Poisson at a rate swept as multiples of the plain path's
     measured capacity.  Plain: one host thread serves requests in arrival
     order, each as tk_matvec_host (copy in, one fused launch, copy out, sync).
     Server: the same thread submits each request at its arrival time to
-    tk_server (continuous batching).  Latency = completion - scheduled
+    tk_server (continuous batching; staged through the server's HBM pool, and
+    with --serve-zero-copy also a server that reads the pinned buffers in
+    place).  Latency = completion - scheduled
     arrival; throughput = output polynomials / (last completion - start)."""
     import ctypes
 
@@ -507,7 +511,10 @@ def run_serve(args):
     tmpl = []
     for _ in range(T):
         k, n = int(r.integers(2, 5)), int(r.integers(1, 65))
-        A, sv, e = pinned((n, k, k, 256)), pinned((n, k, 256)), pinned((n, k, 256))
+        blk = pinned((n * (k * k + 2 * k), 256))       # one request message: A | s | e
+        A = blk[:n * k * k].reshape(n, k, k, 256)
+        sv = blk[n * k * k:n * (k * k + k)].reshape(n, k, 256)
+        e = blk[n * (k * k + k):].reshape(n, k, 256)
         A[...] = r.integers(0, Q, size=A.shape)
         sv[...] = r.integers(0, Q, size=sv.shape)
         e[...] = r.integers(0, Q, size=e.shape)
@@ -539,24 +546,20 @@ def run_serve(args):
     def pct(v, p):
         return float(np.percentile(np.asarray(v) * 1e6, p))
 
-    srv = tk.Server(hbm_budget_bytes=1 << 30, max_inflight_requests=1024, idle_exit_seconds=0.05)
-    ticket = ctypes.c_uint64()
-    for t in tmpl:                      # server warm-up
-        a, b_, c, d = t["ptrs"]
-        if L.tk_server_submit(srv._h, t["k"], t["n"], a, b_, c, d, ctypes.byref(ticket)):
-            raise tk.TKError(1, "submit")
-        srv.wait(ticket.value)
-        srv.release(ticket.value)
-    points = []
+    mults = [float(x) for x in args.serve_rates.split(",")]
+    # one arrival sequence per rate, shared by every arm
+    runs = []
+    for mult in mults:
+        arr = np.cumsum(r.exponential(1.0 / (mult * cap), size=args.serve_requests))
+        which = r.integers(0, T, size=args.serve_requests)
+        runs.append((mult, arr, which, int(polys[which].sum())))
+    points = [{"offered_x_plain_capacity": m, "offered_requests_per_s": m * cap,
+               "requests": len(a), "polys": p} for m, a, _, p in runs]
     sampler = ClockSampler(0)
     sampler.start()
-    for mult in [float(x) for x in args.serve_rates.split(",")]:
-        rate = mult * cap
-        nreq = args.serve_requests
-        arr = np.cumsum(r.exponential(1.0 / rate, size=nreq))
-        which = r.integers(0, T, size=nreq)
-        tot_polys = int(polys[which].sum())
-        # plain per-request launch, FIFO
+    # plain per-request launch, FIFO, with no server alive
+    for pt, (mult, arr, which, tot_polys) in zip(points, runs):
+        nreq = len(arr)
         lat = np.empty(nreq)
         base = pc() + 1e-3
         for i in range(nreq):
@@ -564,39 +567,62 @@ def run_serve(args):
             spin_until(ta)
             plain_one(tmpl[which[i]])
             lat[i] = pc() - ta
-        plain_end = max(base + arr[i] + lat[i] for i in range(nreq))
-        plain = {"p50_us": pct(lat, 50), "p99_us": pct(lat, 99),
-                 "polys_per_s": tot_polys / (plain_end - base),
-                 "requests_per_s": nreq / (plain_end - base)}
-        # server
-        lag = np.empty(nreq)
-        tickets = np.empty(nreq, dtype=np.uint64)
-        base = pc() + 1e-3
-        for i in range(nreq):
-            ta = base + arr[i]
-            spin_until(ta)
-            t = tmpl[which[i]]
+        end = base + float(np.max(arr + lat))
+        pt["plain"] = {"p50_us": pct(lat, 50), "p99_us": pct(lat, 99),
+                       "polys_per_s": tot_polys / (end - base),
+                       "requests_per_s": nreq / (end - base)}
+    # each server arm alone: its device loop holds every SM while it runs
+    arms = {"server": dict(zero_copy=False)}
+    if args.serve_zero_copy:
+        arms["server_zero_copy"] = dict(zero_copy=True)
+    ticket = ctypes.c_uint64()
+    stats = {}
+    for name, kw in arms.items():
+        srv = tk.Server(hbm_budget_bytes=1 << 30, max_inflight_requests=1024,
+                        idle_exit_seconds=0.05, **kw)
+        for t in tmpl:                  # warm-up
             a, b_, c, d = t["ptrs"]
-            rc = L.tk_server_submit(srv._h, t["k"], t["n"], a, b_, c, d, ctypes.byref(ticket))
-            lag[i] = pc() - ta
-            if rc:
-                raise tk.TKError(rc, "submit")
-            tickets[i] = ticket.value
-        slat = np.empty(nreq)
-        for i in range(nreq):
-            srv.wait(int(tickets[i]), timeout=60)
-            slat[i] = lag[i] + srv.latency(int(tickets[i]))
-            srv.release(int(tickets[i]))
-        srv_end = base + max(arr[i] + slat[i] for i in range(nreq))
-        server = {"p50_us": pct(slat, 50), "p99_us": pct(slat, 99),
-                  "polys_per_s": tot_polys / (srv_end - base),
-                  "requests_per_s": nreq / (srv_end - base),
-                  "submit_lag_p99_us": pct(lag, 99)}
-        points.append({"offered_x_plain_capacity": mult, "offered_requests_per_s": rate,
-                       "requests": nreq, "polys": tot_polys, "plain": plain, "server": server})
+            if L.tk_server_submit(srv._h, t["k"], t["n"], a, b_, c, d, ctypes.byref(ticket)):
+                raise tk.TKError(1, "submit")
+            srv.wait(ticket.value)
+            srv.release(ticket.value)
+        for t in tmpl:
+            assert (t["o_srv"] == t["o_plain"]).all(), name
+        st0 = srv.stats()
+        for pt, (mult, arr, which, tot_polys) in zip(points, runs):
+            nreq = len(arr)
+            lag = np.empty(nreq)
+            tickets = np.empty(nreq, dtype=np.uint64)
+            base = pc() + 1e-3
+            for i in range(nreq):
+                ta = base + arr[i]
+                spin_until(ta)
+                t = tmpl[which[i]]
+                a, b_, c, d = t["ptrs"]
+                rc = L.tk_server_submit(srv._h, t["k"], t["n"], a, b_, c, d,
+                                        ctypes.byref(ticket))
+                lag[i] = pc() - ta
+                if rc:
+                    raise tk.TKError(rc, "submit")
+                tickets[i] = ticket.value
+            slat = np.empty(nreq)
+            for i in range(nreq):
+                srv.wait(int(tickets[i]), timeout=60)
+                slat[i] = lag[i] + srv.latency(int(tickets[i]))
+                srv.release(int(tickets[i]))
+            end = base + float(np.max(arr + slat))
+            st = srv.stats()
+            split = {f"mean_{x}_us": (st[f"{x}_ns"] - st0[f"{x}_ns"]) / 1e3 /
+                     max(1, st["requests_done"] - st0["requests_done"])
+                     for x in ("queue", "device", "return")}
+            st0 = st
+            pt[name] = {"p50_us": pct(slat, 50), "p99_us": pct(slat, 99),
+                        "polys_per_s": tot_polys / (end - base),
+                        "requests_per_s": nreq / (end - base),
+                        "submit_lag_p99_us": pct(lag, 99), **split}
+        stats[name] = srv.stats()
+        srv.close()
     clocks = sampler.stop()
-    stats = srv.stats()
-    srv.close()
     exact = all((t["o_srv"] == t["o_plain"]).all() for t in tmpl)
     assert tk.device_status(0) == 0
     top = points[-1]
@@ -608,7 +634,7 @@ def run_serve(args):
         "points": points, "server_outputs_equal_plain": bool(exact),
         "server_stats": stats, "clocks": clocks,
         "config": {"workload": "requests of 1-64 matrix-vector jobs, k ~ U{2,3,4}, "
-                               "coefficients uniform [0,q), pinned host buffers",
+                               "coefficients uniform [0,q), pinned host buffers (A|s|e contiguous)",
                    "templates": T, "mode": "fused"},
         "dtype": "int16", "data": "synthetic",
     }), flush=True)

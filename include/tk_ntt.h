@@ -100,30 +100,49 @@ typedef struct tk_matvec_batch {
   int16_t *out;
 } tk_matvec_batch;
 int tk_matvec(const tk_matvec_batch *batches, int nbatches, tk_stream_t stream);
-/* tk_matvec on HOST buffers, synchronous: copies A, s, e in, runs the same
- * kernels, copies out back (the plain per-request launch).  Uses a device
+/* tk_matvec on HOST buffers, synchronous: copies A, s, e in (one copy when
+ * they are contiguous, A then s then e), runs the same kernels, copies out
+ * back (the plain per-request launch).  Uses a device
  * staging buffer per device that grows to the largest call (at most 8 GiB);
  * calls on one device are serialised.  out may alias s. */
 int tk_matvec_host(const tk_matvec_batch *batches, int nbatches);
 
 /* ---- serving loop (continuous batching) ----------------------------------
- * A server owns hbm_budget_bytes of device memory and a persistent device
- * loop that runs matrix-vector jobs (tk_matvec semantics) from a device-
- * resident job ring.  tk_server_submit queues a request of njobs jobs of one
- * k whose buffers are HOST memory (A: njobs*k*k, s/e/out: njobs*k
- * polynomials; e may be NULL); requests are admitted in arrival order as pool
- * memory and request slots free up, and their jobs run alongside jobs already
- * on the GPU.  Results land in out before the ticket completes.  All host
- * waits take a timeout; the device loop exits after idle_exit_seconds without
- * work and is relaunched on demand.  While it runs, the device loop occupies
- * every SM.  No reference counterpart (the reference times fixed batches).
- * Buffers passed to submit must stay valid until the ticket completes. */
+ * A server runs matrix-vector jobs (tk_matvec semantics) from a device-
+ * resident job ring through a persistent device loop.  tk_server_submit
+ * queues a request of njobs jobs of one k whose buffers are HOST memory
+ * (A: njobs*k*k, s/e/out: njobs*k polynomials; e may be NULL; A, s, e laid
+ * out back to back travel in one copy).  Requests are admitted in arrival order as request slots (and, for staged requests, pool
+ * memory) free up; their jobs run alongside jobs already on the GPU, and
+ * results land in out before the ticket completes.
+ *   - inputs: A, s, e are copied into the server's device pool of
+ *     hbm_budget_bytes (admission waits for room), or, with zero_copy = 1
+ *     and all three in page-locked host memory the device can address
+ *     (cudaHostAlloc / cudaHostRegister), read in place over PCIe (uncached
+ *     reads: slower than one bulk copy for all but tiny requests);
+ *   - outputs: written in place when out is such memory (posted PCIe
+ *     writes), else produced in the pool and copied back.
+ * All host waits take a timeout; the device loop exits after
+ * idle_exit_seconds without work and is relaunched on demand.  While it runs
+ * it occupies every SM.  No reference counterpart (the reference times fixed
+ * batches).  Buffers passed to submit must stay valid until the ticket
+ * completes. */
 typedef struct tk_server tk_server;
 typedef struct tk_server_config {
-  size_t hbm_budget_bytes;    /* device pool for admitted requests (0: 1 GiB) */
+  size_t hbm_budget_bytes;    /* device pool for staged requests (0: 1 GiB) */
   int max_inflight_requests;  /* request slots (0: 1024) */
   double idle_exit_seconds;   /* device loop idle limit (0: 0.02 s) */
+  int zero_copy;              /* 1: read/write page-locked buffers in place */
 } tk_server_config;
+/* Cumulative counters; the *_ns sums split each completed request's latency
+ * into queueing (submit -> admitted), device (admitted -> last job done) and
+ * return (-> outputs in host memory) time. */
+typedef struct tk_server_counters {
+  unsigned long long requests_done, jobs_done, device_loop_launches;
+  unsigned long long direct_requests, staged_requests;  /* inputs in place / staged */
+  unsigned long long direct_outputs;                    /* outputs written in place */
+  unsigned long long queue_ns, device_ns, return_ns;
+} tk_server_counters;
 int tk_server_create(int device, const tk_server_config *cfg, tk_server **out);
 int tk_server_submit(tk_server *srv, int k, size_t njobs, const int16_t *A, const int16_t *s,
                      const int16_t *e, int16_t *out, uint64_t *ticket);
@@ -133,7 +152,7 @@ int tk_server_wait(tk_server *srv, uint64_t ticket, double timeout_s);
 int tk_server_query(tk_server *srv, uint64_t ticket, int *done, double *latency_s);
 /* Forget a completed ticket. */
 int tk_server_release(tk_server *srv, uint64_t ticket);
-int tk_server_stats(tk_server *srv, unsigned long long *jobs_done, unsigned long long *launches);
+int tk_server_stats(tk_server *srv, tk_server_counters *out);
 /* Waits (up to timeout_s) for outstanding requests, stops the loop, frees all. */
 int tk_server_destroy(tk_server *srv, double timeout_s);
 

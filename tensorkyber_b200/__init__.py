@@ -40,7 +40,14 @@ class MatvecBatch(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     """Mirror of tk_server_config (include/tk_ntt.h)."""
     _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_inflight_requests", ctypes.c_int),
-                ("idle_exit_seconds", ctypes.c_double)]
+                ("idle_exit_seconds", ctypes.c_double), ("zero_copy", ctypes.c_int)]
+
+
+class ServerCounters(ctypes.Structure):
+    """Mirror of tk_server_counters (include/tk_ntt.h)."""
+    _fields_ = [(n, ctypes.c_ulonglong) for n in (
+        "requests_done", "jobs_done", "device_loop_launches", "direct_requests",
+        "staged_requests", "direct_outputs", "queue_ns", "device_ns", "return_ns")]
 
 
 class TKError(RuntimeError):
@@ -127,8 +134,7 @@ def lib() -> ctypes.CDLL:
     L.tk_server_query.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_double)]
     L.tk_server_release.argtypes = [vp, ctypes.c_uint64]
-    L.tk_server_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong),
-                                  ctypes.POINTER(ctypes.c_ulonglong)]
+    L.tk_server_stats.argtypes = [vp, ctypes.POINTER(ServerCounters)]
     L.tk_server_destroy.argtypes = [vp, ctypes.c_double]
     for f in ("tk_server_create", "tk_server_submit", "tk_server_wait", "tk_server_query",
               "tk_server_release", "tk_server_stats", "tk_server_destroy"):
@@ -263,11 +269,15 @@ class Server:
 
     Requests are numpy int16 arrays in host memory: A (njobs, k, k, 256),
     s / e (njobs, k, 256), out (njobs, k, 256); they must stay alive until the
-    request completes (the object keeps references until release)."""
+    request completes (the object keeps references until release).  With
+    zero_copy, arrays in page-locked memory (e.g. torch.empty(...,
+    pin_memory=True).numpy()) are read and written in place by the device loop;
+    everything else is staged through the server's HBM pool."""
 
     def __init__(self, hbm_budget_bytes=1 << 30, max_inflight_requests=1024,
-                 idle_exit_seconds=0.02, device=0):
-        cfg = ServerConfig(hbm_budget_bytes, max_inflight_requests, idle_exit_seconds)
+                 idle_exit_seconds=0.02, device=0, zero_copy=False):
+        cfg = ServerConfig(hbm_budget_bytes, max_inflight_requests, idle_exit_seconds,
+                           int(zero_copy))
         h = ctypes.c_void_p()
         _check(lib().tk_server_create(device, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
@@ -298,9 +308,9 @@ class Server:
         self._keep.pop(ticket, None)
 
     def stats(self):
-        jobs, launches = ctypes.c_ulonglong(), ctypes.c_ulonglong()
-        _check(lib().tk_server_stats(self._h, ctypes.byref(jobs), ctypes.byref(launches)))
-        return {"jobs_done": jobs.value, "device_loop_launches": launches.value}
+        c = ServerCounters()
+        _check(lib().tk_server_stats(self._h, ctypes.byref(c)))
+        return {n: getattr(c, n) for n, _ in ServerCounters._fields_}
 
     def close(self, timeout: float = 60.0) -> None:
         if self._h:

@@ -1,6 +1,8 @@
 // tk_api.cu -- the C ABI (include/tk_ntt.h): argument checks, per-device set-up,
 // dispatch to the sm_100a kernels, and the chunked host-memory path.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <string.h>
@@ -267,6 +269,33 @@ int run_host(bool inverse, int16_t* polys, size_t npoly) {
 }  // namespace
 
 namespace tk {
+bool host_span_one_copy(const void* p, size_t bytes) {
+  static PFN_cuPointerGetAttribute_v4000 get_attr = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    return cudaGetDriverEntryPoint("cuPointerGetAttribute", &f, cudaEnableDefault, &q) ==
+                       cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess
+               ? (PFN_cuPointerGetAttribute_v4000)f
+               : nullptr;
+  }();
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type == cudaMemoryTypeUnregistered) return true;
+  if (a.type != cudaMemoryTypeHost || !get_attr) return false;
+  // page-locked: the span must stay inside the allocation
+  CUdeviceptr start = 0;
+  size_t size = 0;
+  const CUdeviceptr dp = (CUdeviceptr)(a.devicePointer ? a.devicePointer : p);
+  if (get_attr(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, dp) != CUDA_SUCCESS ||
+      get_attr(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, dp) != CUDA_SUCCESS)
+    return false;
+  return dp >= start && dp + bytes <= start + size;
+}
+
 int api_device_info(int device, DeviceInfo** info) {
   if (device < 0 || device >= kMaxDevices) return TK_ERR_INVALID_VALUE;
   return ensure_ready(device, info);
@@ -411,7 +440,7 @@ int tk_matvec_host(const tk_matvec_batch* batches, int nbatches) {
   for (int b = 0; b < nbatches; b++) {
     const tk_matvec_batch& B = batches[b];
     const size_t vb = B.njobs * (size_t)B.k * 512u;
-    need += up(vb * (size_t)B.k) + up(vb) * (B.e ? 3 : 2);
+    need += up(vb * (size_t)B.k + vb * (B.e ? 3 : 2));
   }
   if (need > kMaxStage) {
     set_msg("tk_matvec_host: batch list above the 8 GiB staging limit");
@@ -444,15 +473,24 @@ int tk_matvec_host(const tk_matvec_batch* batches, int nbatches) {
     tk_matvec_batch& D = dev_batches[(size_t)b];
     D = B;
     if (B.njobs == 0) continue;
+    // staging block A | s | e | out, unpadded (whole 512-byte polynomials), so
+    // inputs the caller keeps contiguous arrive in one copy
     const size_t vb = B.njobs * (size_t)B.k * 512u, ab = vb * (size_t)B.k;
     int16_t* dA = (int16_t*)(S.mv_stage + off);
-    int16_t* ds = (int16_t*)(S.mv_stage + off + up(ab));
-    int16_t* dout = (int16_t*)(S.mv_stage + off + up(ab) + up(vb));
-    int16_t* de = B.e ? (int16_t*)(S.mv_stage + off + up(ab) + 2 * up(vb)) : nullptr;
-    off += up(ab) + up(vb) * (B.e ? 3 : 2);
-    e = cudaMemcpyAsync(dA, B.A, ab, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(ds, B.s, vb, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && de) e = cudaMemcpyAsync(de, B.e, vb, cudaMemcpyHostToDevice, st);
+    int16_t* ds = (int16_t*)(S.mv_stage + off + ab);
+    int16_t* de = B.e ? (int16_t*)(S.mv_stage + off + ab + vb) : nullptr;
+    int16_t* dout = (int16_t*)(S.mv_stage + off + ab + vb * (B.e ? 2 : 1));
+    off += up(ab + vb * (B.e ? 3 : 2));
+    const bool packed = (const uint8_t*)B.s == (const uint8_t*)B.A + ab &&
+                        (!B.e || (const uint8_t*)B.e == (const uint8_t*)B.s + vb) &&
+                        tk::host_span_one_copy(B.A, ab + vb * (B.e ? 2 : 1));
+    if (packed) {
+      e = cudaMemcpyAsync(dA, B.A, ab + vb * (B.e ? 2 : 1), cudaMemcpyHostToDevice, st);
+    } else {
+      e = cudaMemcpyAsync(dA, B.A, ab, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(ds, B.s, vb, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess && de) e = cudaMemcpyAsync(de, B.e, vb, cudaMemcpyHostToDevice, st);
+    }
     D.A = dA;
     D.s = ds;
     D.e = de;

@@ -60,8 +60,9 @@ cudaError_t launch_matvec(int k, size_t njobs, const int16_t* A, const int16_t* 
                           long long chunk_vec_polys);
 
 // ---- serving loop (device side in tk_matvec.cu, host side in tk_serve.cpp) ----
-// One job descriptor of the device-resident ring (64 bytes).
-struct ServeJob {
+// One job descriptor of the job ring (64 bytes; the ring lives in mapped
+// page-locked host memory).
+struct alignas(64) ServeJob {
   const int16_t* A;
   const int16_t* s;
   const int16_t* e;
@@ -72,25 +73,37 @@ struct ServeJob {
   uint32_t gen;    // request generation written to the completion flag
   uint64_t pad[2];
 };
-// Device-memory control block.  head: jobs claimed (device atomics); tail:
-// jobs published (written by the host with stream-ordered copy-engine
-// memsets); both count modulo 2^32 and are compared as (int)(tail - head);
-// stop: set by the host to end the loop.
-struct ServeCtl {
-  unsigned int head;
-  unsigned int tail;
-  unsigned int stop;
-  unsigned int pad;
+// Device-memory control block, one 128-byte line per writer: head (claimed
+// jobs, device compare-and-swap), then the host-written words (tail =
+// published jobs, stream-written; stop) with the device's closing flag, then
+// the time of the latest claim.  head and tail count modulo 2^32 and are
+// compared as (int)(tail - head).
+struct alignas(128) ServeCtl {
+  unsigned int head;  // next job to claim (device compare-and-swap)
+  unsigned int pad0[31];
+  unsigned int tail;     // jobs published (host)
+  unsigned int stop;     // host: end the loop now
+  unsigned int closing;  // device: the loop is leaving (host clears)
+  unsigned int pad1[29];
+  unsigned long long last_claim_ns;  // globaltimer of the latest claim
+  unsigned long long pad2[15];
 };
-// Launches the persistent serving kernel.  req_ctr: per-slot done counters
-// (device memory); req_flag: per-slot completion flags in mapped pinned host
-// memory; idle_ns: the loop exits after this long without a claimable job.
+// Launches the persistent serving kernel.  ring: the job ring (mapped host
+// memory); req_ctr: per-slot done counters (device memory); req_flag: per-slot
+// completion flags in mapped pinned host memory; idle_ns: the loop exits after
+// this long without a claim anywhere.
 cudaError_t launch_serve(const ServeJob* ring, uint32_t ring_mask, ServeCtl* ctl,
                          unsigned int* req_ctr, unsigned int* req_flag, unsigned long long idle_ns,
                          const DeviceInfo& info, cudaStream_t stream);
 
 // Per-device state of the API layer (set-up on first use), for other units.
 int api_device_info(int device, DeviceInfo** info);
+
+// True when one host<->device copy may cover host bytes [p, p + bytes): the
+// range starts in pageable memory, or lies inside one page-locked
+// allocation (a copy that runs from one page-locked allocation into the next
+// is not valid).  Needs the device's context current on the calling thread.
+bool host_span_one_copy(const void* p, size_t bytes);
 
 // Kernel-side error flags (bounded waits that gave up), read and reset.
 cudaError_t read_and_clear_status(unsigned* flags);

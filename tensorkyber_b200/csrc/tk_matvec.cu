@@ -156,21 +156,24 @@ struct WarpRegs {
   uint32_t zr[4];
 };
 
-// Global loads of a job's inputs.  kL2Only (the serving loop, whose memory
-// pool is reused by later requests) reads at L2 only, so an L1 line left from
-// an earlier request can never be returned.
-template <bool kL2Only>
+// Global loads of a job's inputs.  kLoad 0: streaming (__ldcs, tk_matvec);
+// 1: volatile (__ldcv, the serving loop).  Serving inputs are either pool
+// memory reused by later requests or a caller's pinned host buffers read in
+// place, whose contents the host may rewrite between requests while the loop
+// keeps running: ld.cv never returns a stale L1 line, and for system memory
+// it discards a matching L2 line and fetches again.
+template <int kLoad>
 __device__ __forceinline__ uint4 job_ld16(const void* p) {
-  return kL2Only ? __ldcg((const uint4*)p) : __ldcs((const uint4*)p);
+  return kLoad ? __ldcv((const uint4*)p) : __ldcs((const uint4*)p);
 }
-template <bool kL2Only>
+template <int kLoad>
 __device__ __forceinline__ uint32_t job_ld4(const void* p) {
-  return kL2Only ? __ldcg((const uint32_t*)p) : __ldcs((const uint32_t*)p);
+  return kLoad ? __ldcv((const uint32_t*)p) : __ldcs((const uint32_t*)p);
 }
 
 // One job of width k (2..4) on this warp.  rows/rowp: the warp's 8 x 528-byte
 // buffer (smem address / pointer).
-template <bool kL2Only>
+template <int kLoad>
 __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
                                           const int16_t* __restrict__ s,
                                           const int16_t* __restrict__ e, int16_t* __restrict__ out,
@@ -190,7 +193,7 @@ __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
 #pragma unroll
   for (int j = 0; j < 4; j++)
     if (j < k) {
-      const uint4 v = job_ld16<kL2Only>(s + j * 256 + 8 * lane);
+      const uint4 v = job_ld16<kLoad>(s + j * 256 + 8 * lane);
       *(uint4*)(rowp + j * kRowBytes + 16 * lane) = v;
     }
   __syncwarp();
@@ -239,7 +242,7 @@ __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
 #pragma unroll
       for (int i = 0; i < 4; i++)
         if (i < k) {
-          const uint4 av = job_ld16<kL2Only>(A + (i * k + j) * 256 + 8 * lane);
+          const uint4 av = job_ld16<kLoad>(A + (i * k + j) * 256 + 8 * lane);
           const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
 #pragma unroll
           for (int u = 0; u < 4; u++) {
@@ -284,10 +287,10 @@ __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
       uint32_t add[4] = {0, 0, 0, 0};
       if (e) {
         const uint32_t* ew = (const uint32_t*)(e + j * 256) + 8 * g8 + q4;
-        add[0] = job_ld4<kL2Only>(ew);
-        add[1] = job_ld4<kL2Only>(ew + 4);
-        add[2] = job_ld4<kL2Only>(ew + 64);
-        add[3] = job_ld4<kL2Only>(ew + 68);
+        add[0] = job_ld4<kLoad>(ew);
+        add[1] = job_ld4<kLoad>(ew + 4);
+        add[2] = job_ld4<kLoad>(ew + 64);
+        add[3] = job_ld4<kLoad>(ew + 68);
       }
       uint32_t b[4];
       ldsm_x4_t(rows + j * kRowBytes + ldt_off, b[0], b[1], b[2], b[3]);
@@ -343,66 +346,156 @@ __global__ void __launch_bounds__(32 * kFusedWarps)
     while (b + 1 < args.nb && job >= args.first[b + 1]) b++;
     const int k = args.k[b];
     const size_t t = (size_t)(job - args.first[b]);
-    fused_job<false>(k, args.A[b] + t * k * k * 256, args.s[b] + t * k * 256,
+    fused_job<0>(k, args.A[b] + t * k * k * 256, args.s[b] + t * k * 256,
               args.e[b] ? args.e[b] + t * k * 256 : nullptr, args.out[b] + t * k * 256, rows, rowp,
               C, R, lane);
   }
 }
 
 // ============================================================================
-// Serving loop: a persistent kernel whose warps claim published jobs from the
-// device-resident ring (compare-and-swap on head only while head < tail, so an
-// unpublished slot is never claimed and the loop may exit at any idle point),
-// run fused_job on them, and count completions per request; the warp that
-// completes a request fences its outputs system-wide and writes the request's
-// generation into the request's flag in mapped host memory.  Every wait is
-// bounded: a warp leaves the loop after idle_ns without a claimable job, or
-// as soon as the host sets ctl->stop.
+// Serving loop: a persistent kernel, one CTA of kServeWarps warps per SM, that
+// claims published jobs from the device-resident ring, runs fused_job on them
+// and counts completions per request; the warp that completes a request
+// fences its outputs system-wide and writes the request's generation into the
+// request's flag in mapped host memory.
+//
+// Job descriptors live in a ring in mapped page-locked host memory (written
+// by the host, read here once per claimed job).  Claiming is per CTA.  An idle warp marks itself in s_idle and watches its
+// shared-memory mailbox; one idle warp at a time (s_lock) acts as the CTA's
+// poller: it reads the global head and tail and, while head < tail, claims
+// min(idle warps, tail - head) jobs with one compare-and-swap on head and
+// hands them to the idle warps' mailboxes (itself included).  An unpublished
+// slot is never claimed, so the loop may stop at any idle point.  With one
+// poller per SM the head line sees 148 pollers, not thousands of warps.
+//
+// Every wait is bounded.  The loop leaves as a whole: once no CTA has claimed
+// a job for idle_ns (ctl->last_claim_ns) a poller sets ctl->closing, and
+// every CTA's poller then tells its warps to leave (a warp finishes a claimed
+// job first).  ctl->stop from the host ends it the same way.  The host clears
+// closing before a relaunch.  Idle polling backs off from 128 ns to 2 us.
 // ============================================================================
-__global__ void __launch_bounds__(32 * kFusedWarps)
+constexpr int kServeWarps = 16;
+
+__device__ __forceinline__ uint4 shfl_u4(const uint4& v, int src) {
+  return make_uint4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+                    __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
+}
+constexpr int kServeSmem = kFusedConstBytes + kServeWarps * kFusedWarpBytes;
+constexpr unsigned long long kNoJob = ~0ull, kExitJob = ~0ull - 1;
+
+__device__ __forceinline__ unsigned int ld_relaxed_u32(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__global__ void __launch_bounds__(32 * kServeWarps, 1)
     k_serve(const ServeJob* __restrict__ ring, uint32_t ring_mask, ServeCtl* ctl,
             unsigned int* req_ctr, unsigned int* req_flag, unsigned long long idle_ns) {
   extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ unsigned long long s_job[kServeWarps];  // mailbox: job, kNoJob or kExitJob
+  __shared__ unsigned int s_idle;                    // warps waiting for a job
+  __shared__ int s_lock, s_exit;
   FusedConsts* C = (FusedConsts*)smem;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint8_t* rowp = smem + kFusedConstBytes + warp * kFusedWarpBytes;
   const uint32_t rows = smem_u32(rowp);
+  if (threadIdx.x < kServeWarps) s_job[threadIdx.x] = kNoJob;
+  if (threadIdx.x == 0) {
+    s_idle = 0;
+    s_lock = 0;
+    s_exit = 0;
+  }
   fused_load_consts(C);
   WarpRegs R;
   fused_warp_regs(R, lane);
   __syncthreads();
-  volatile unsigned int* stop = &ctl->stop;
+  const unsigned long long t_start = globaltimer_ns();
+  volatile unsigned long long* box = &s_job[warp];
   while (true) {
-    unsigned long long got = ~0ull;
+    unsigned long long got = kNoJob;
     if (lane == 0) {
-      unsigned long long t0 = globaltimer_ns();
+      atomicOr(&s_idle, 1u << warp);
+      unsigned int backoff = 128;
       while (true) {
-        unsigned int h, t;
-        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(h) : "l"(&ctl->head) : "memory");
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(t) : "l"(&ctl->tail) : "memory");
-        if ((int)(t - h) > 0) {
-          if (atomicCAS(&ctl->head, h, h + 1) == h) {
-            got = h;
-            break;
-          }
+        const unsigned long long mine = *box;
+        if (mine != kNoJob) {
+          *box = kNoJob;
+          got = mine;
+          break;
+        }
+        if (atomicCAS(&s_lock, 0, 1) != 0) {  // another warp is polling
+          __nanosleep(64);
           continue;
         }
-        if (*stop) break;
-        if (globaltimer_ns() - t0 > idle_ns) break;
-        __nanosleep(500);
+        // this warp polls for the CTA
+        bool claimed = false;
+        if (*(volatile int*)&s_exit || ld_relaxed_u32(&ctl->closing) || ld_relaxed_u32(&ctl->stop)) {
+          *(volatile int*)&s_exit = 1;
+          *box = kExitJob;
+        } else {
+          const unsigned int h = ld_relaxed_u32(&ctl->head);
+          unsigned int t;
+          asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(t) : "l"(&ctl->tail) : "memory");
+          const int avail = (int)(t - h);
+          if (avail > 0) {
+            const unsigned int idle = *(volatile unsigned int*)&s_idle;
+            const int n = min(avail, __popc(idle));
+            if (atomicCAS(&ctl->head, h, h + (unsigned)n) == h) {
+              asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(&ctl->last_claim_ns),
+                           "l"(globaltimer_ns())
+                           : "memory");
+              unsigned int m = idle, given = 0;
+              for (int i = 0; i < n; i++) {
+                const int w = __ffs(m) - 1;
+                m &= m - 1;
+                given |= 1u << w;
+                ((volatile unsigned long long*)s_job)[w] = (unsigned long long)(h + (unsigned)i);
+              }
+              atomicAnd(&s_idle, ~given);
+            }
+            claimed = true;  // claimed, or lost the race: poll again at once
+          } else {
+            unsigned long long last;
+            asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(last)
+                         : "l"(&ctl->last_claim_ns)
+                         : "memory");
+            // signed: another SM's timer may run slightly ahead of this one's
+            const long long since =
+                (long long)(globaltimer_ns() - (last > t_start ? last : t_start));
+            if (since > (long long)idle_ns) {
+              asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(&ctl->closing), "r"(1u)
+                           : "memory");
+              *(volatile int*)&s_exit = 1;
+              *box = kExitJob;
+            }
+          }
+        }
+        __threadfence_block();
+        atomicExch(&s_lock, 0);
+        if (!claimed && *box == kNoJob) {
+          __nanosleep(backoff);
+          if (backoff < 2048) backoff <<= 1;
+        }
       }
+      __threadfence_block();
     }
     got = __shfl_sync(0xffffffffu, got, 0);
-    if (got == ~0ull) break;  // warp-uniform exit
-    const ServeJob* J = ring + (got & ring_mask);
-    const int16_t* A = (const int16_t*)__ldcg((const unsigned long long*)&J->A);
-    const int16_t* sv = (const int16_t*)__ldcg((const unsigned long long*)&J->s);
-    const int16_t* ev = (const int16_t*)__ldcg((const unsigned long long*)&J->e);
-    int16_t* out = (int16_t*)__ldcg((const unsigned long long*)&J->out);
-    const uint4 meta = __ldcg((const uint4*)&J->k);  // k, req, njobs, gen
-    fused_job<true>((int)meta.x, A, sv, ev, out, rows, rowp, C, R, lane);
+    if (got == kExitJob) break;  // warp-uniform exit
+    // the descriptor, from the ring in host memory: lanes 0..2 fetch its
+    // 16-byte parts (uncached: the host rewrites entries as the ring wraps)
+    uint4 part = make_uint4(0, 0, 0, 0);
+    if (lane < 3) part = __ldcv((const uint4*)(ring + (got & ring_mask)) + lane);
+    const uint4 p0 = shfl_u4(part, 0), p1 = shfl_u4(part, 1);
+    const uint4 meta = shfl_u4(part, 2);  // k, req, njobs, gen
+    const int16_t* A = (const int16_t*)(((unsigned long long)p0.y << 32) | p0.x);
+    const int16_t* sv = (const int16_t*)(((unsigned long long)p0.w << 32) | p0.z);
+    const int16_t* ev = (const int16_t*)(((unsigned long long)p1.y << 32) | p1.x);
+    int16_t* out = (int16_t*)(((unsigned long long)p1.w << 32) | p1.z);
+    fused_job<1>((int)meta.x, A, sv, ev, out, rows, rowp, C, R, lane);
     if (lane == 0) {
-      __threadfence();
+      // outputs may be host memory: order them system-wide before counting
+      __threadfence_system();
       const unsigned int done = atomicAdd(&req_ctr[meta.y], 1u) + 1u;
       if (done == meta.z) {
         // every job of the request has counted: reset the counter for the
@@ -424,14 +517,11 @@ cudaError_t launch_serve(const ServeJob* ring, uint32_t ring_mask, ServeCtl* ctl
   static cudaError_t attr_err = cudaSuccess;
   std::call_once(once, [] {
     attr_err = cudaFuncSetAttribute(k_serve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    kFusedSmem);
+                                    kServeSmem);
   });
   if (attr_err != cudaSuccess) return attr_err;
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_serve, 32 * kFusedWarps, kFusedSmem);
-  const unsigned blocks = (unsigned)(info.num_sms * (per_sm > 0 ? per_sm : 1));
-  k_serve<<<blocks, 32 * kFusedWarps, kFusedSmem, stream>>>(ring, ring_mask, ctl, req_ctr, req_flag,
-                                                           idle_ns);
+  k_serve<<<(unsigned)info.num_sms, 32 * kServeWarps, kServeSmem, stream>>>(
+      ring, ring_mask, ctl, req_ctr, req_flag, idle_ns);
   return cudaGetLastError();
 }
 

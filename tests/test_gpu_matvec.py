@@ -113,6 +113,14 @@ def test_matvec_host_matches_device(tk, cuda, oracle, mode):
     tk.matvec_host(items)
     for (k, A, s, e, out), x in zip(items, expect):
         assert (canon(out) == canon(x)).all()
+    k, A, s, e, out = items[1]                           # A, s, e back to back: one copy
+    buf = np.concatenate([A.ravel(), s.ravel(), e.ravel()])
+    pA = buf[:A.size].reshape(A.shape)
+    ps = buf[A.size:A.size + s.size].reshape(s.shape)
+    pe = buf[A.size + s.size:].reshape(e.shape)
+    out2 = np.zeros_like(s)
+    tk.matvec_host([(k, pA, ps, pe, out2)])
+    assert (out2 == out).all()
     k, A, s, e, out = items[2]
     tk.matvec_host([(k, A, s, None, s)])                 # in place, no addend
     assert (canon(s) == canon(expect[2] - e)).all()

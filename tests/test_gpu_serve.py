@@ -26,6 +26,28 @@ def request(seed, k, n, uniform=False):
     return A, s, e
 
 
+def pinned_copy(a):
+    """a copied into page-locked host memory (read in place by the server)."""
+    import torch
+    p = torch.empty(a.shape, dtype=torch.int16, pin_memory=True).numpy()
+    p[...] = a
+    return p
+
+
+def packed(A, s, e):
+    """A, s, e as views of one contiguous buffer (A then s then e)."""
+    buf = np.empty(A.size + s.size + e.size, dtype=np.int16)
+    pa, ps = buf[:A.size].reshape(A.shape), buf[A.size:A.size + s.size].reshape(s.shape)
+    pe = buf[A.size + s.size:].reshape(e.shape)
+    pa[...], ps[...], pe[...] = A, s, e
+    return pa, ps, pe
+
+
+@pytest.fixture(params=["pageable", "pageable-packed", "pinned", "pinned-zero-copy"])
+def memkind(request):
+    return request.param
+
+
 def oracle_out(oracle, k, A, s, e):
     return np.stack([oracle.matvec_job(k, A[t].reshape(k * k, 256), s[t], e[t])
                      for t in range(A.shape[0])])
@@ -43,15 +65,22 @@ def test_single_request_matches_oracle(tk, cuda, oracle):
             srv.release(t)
 
 
-def test_alone_equals_in_the_mix(tk, cuda, oracle):
-    """48 requests (k in {2,3,4}, 1..64 jobs) from 3 client threads with a
-    small HBM budget, so admission has to wait for memory to free up; then the
-    same requests one at a time.  Outputs must be identical."""
+def test_alone_equals_in_the_mix(tk, cuda, oracle, memkind):
+    """48 requests (k in {2,3,4}, 1..64 jobs) from 3 client threads; then the
+    same requests one at a time.  Outputs must be identical.  Pageable buffers
+    are staged through a small HBM budget, so admission has to wait for memory
+    to free up; pinned buffers are read and written in place."""
     r = rng(99)
     reqs = [(int(r.integers(2, 5)), int(r.integers(1, 65))) for _ in range(48)]
     data = [request(1000 + i, k, n, uniform=True) for i, (k, n) in enumerate(reqs)]
-    mixed = [np.zeros_like(d[1]) for d in data]
-    with tk.Server(hbm_budget_bytes=4 << 20, max_inflight_requests=16) as srv:
+    conv = pinned_copy if memkind.startswith("pinned") else (lambda a: a)
+    zero_copy = memkind == "pinned-zero-copy"
+    data = [tuple(conv(x) for x in d) for d in data]
+    if memkind == "pageable-packed":
+        data = [packed(*d) for d in data]
+    mixed = [conv(np.zeros_like(d[1])) for d in data]
+    with tk.Server(hbm_budget_bytes=4 << 20, max_inflight_requests=16,
+                   zero_copy=zero_copy) as srv:
         errors = []
 
         def client(idx):
@@ -73,6 +102,9 @@ def test_alone_equals_in_the_mix(tk, cuda, oracle):
         assert not errors
         stats = srv.stats()
         assert stats["jobs_done"] == sum(n for _, n in reqs)
+        kind = "direct_requests" if zero_copy else "staged_requests"
+        assert stats[kind] == len(reqs), stats
+        assert stats["direct_outputs"] == (len(reqs) if memkind.startswith("pinned") else 0)
     alone = []
     with tk.Server(hbm_budget_bytes=64 << 20) as srv:
         for i, (k, n) in enumerate(reqs):
@@ -114,3 +146,32 @@ def test_server_rejects_oversized_and_bad_requests(tk, cuda):
         assert L.tk_server_submit(srv._h, 5, 1, s.ctypes.data, s.ctypes.data, None,
                                   out.ctypes.data, ctypes.byref(t)) == 1
         assert L.tk_server_wait(srv._h, 12345, 0.01) == 1
+
+
+def test_pinned_buffers_rewritten_between_requests(tk, cuda, oracle):
+    """The device loop keeps running while the host rewrites a pinned input
+    buffer; the next request must see the new contents (no stale cache line)."""
+    k, n = 3, 8
+    with tk.Server(idle_exit_seconds=1.0, zero_copy=True) as srv:
+        bufs = [pinned_copy(x) for x in request(31, k, n, uniform=True)]
+        out = pinned_copy(np.zeros_like(bufs[1]))
+        for rnd in range(4):
+            A, s, e = request(40 + rnd, k, n, uniform=True)
+            bufs[0][...], bufs[1][...], bufs[2][...] = A, s, e
+            srv.wait(srv.submit(k, *bufs, out))
+            assert (canon(out) == canon(oracle_out(oracle, k, A, s, e))).all(), rnd
+        st = srv.stats()
+        assert st["direct_requests"] == 4 and st["device_loop_launches"] == 1, st
+
+
+def test_pinned_is_staged_without_zero_copy(tk, cuda, oracle):
+    k, n = 2, 5
+    A, s, e = (pinned_copy(x) for x in request(8, k, n, uniform=True))
+    out = pinned_copy(np.zeros_like(s))
+    with tk.Server() as srv:
+        srv.wait(srv.submit(k, A, s, e, out))
+        st = srv.stats()
+        assert st["staged_requests"] == 1 and st["direct_requests"] == 0
+        assert st["direct_outputs"] == 1
+        assert st["queue_ns"] + st["device_ns"] + st["return_ns"] > 0
+    assert (canon(out) == canon(oracle_out(oracle, k, A, s, e))).all()
