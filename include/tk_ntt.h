@@ -106,6 +106,16 @@ int tk_matvec(const tk_matvec_batch *batches, int nbatches, tk_stream_t stream);
  * staging buffer per device that grows to the largest call (at most 8 GiB);
  * calls on one device are serialised.  out may alias s. */
 int tk_matvec_host(const tk_matvec_batch *batches, int nbatches);
+/* tk_matvec_host for callers that must not allocate device memory or streams
+ * (no counterpart in the reference).  Staging is a static device array of
+ * TK_NOALLOC_SCRATCH_BYTES that comes with the library module; a batch list
+ * needing more (A + s + e + out bytes per batch, each rounded up to 256)
+ * returns TK_ERR_TOO_LARGE.  The work runs on `stream` and the call returns
+ * after synchronizing it; at most 16 batches.  Per device, the first call looks
+ * up the array's address (cudaGetSymbolAddress): make it before any stream
+ * capture.  Calls on one device that overlap in time race on the array. */
+#define TK_NOALLOC_SCRATCH_BYTES (4 << 20)
+int tk_matvec_host_noalloc(const tk_matvec_batch *batches, int nbatches, tk_stream_t stream);
 
 /* ---- serving loop (continuous batching) ----------------------------------
  * A server runs matrix-vector jobs (tk_matvec semantics) from a device-

@@ -127,6 +127,9 @@ def lib() -> ctypes.CDLL:
     L.tk_matvec.restype = ctypes.c_int
     L.tk_matvec_host.argtypes = [ctypes.POINTER(MatvecBatch), ctypes.c_int]
     L.tk_matvec_host.restype = ctypes.c_int
+    L.tk_matvec_host_noalloc.argtypes = [ctypes.POINTER(MatvecBatch), ctypes.c_int,
+                                         ctypes.c_void_p]
+    L.tk_matvec_host_noalloc.restype = ctypes.c_int
     vp, u64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)
     L.tk_server_create.argtypes = [ctypes.c_int, ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
     L.tk_server_submit.argtypes = [vp, ctypes.c_int, ctypes.c_size_t, vp, vp, vp, vp, u64p]
@@ -248,6 +251,28 @@ def matvec(batches, stream=None):
                                  e.data_ptr() if e is not None else None, out.data_ptr()))
     arr = (MatvecBatch * len(items))(*items)
     _check(lib().tk_matvec(arr, len(items), _stream_ptr(stream)))
+
+
+NOALLOC_SCRATCH_BYTES = 4 << 20
+
+
+def _host_batches(batches):
+    items = []
+    for k, A, s, e, out in batches:
+        n = _host_arr(s) // k
+        if _host_arr(A) != n * k * k or _host_arr(out) != n * k or (
+                e is not None and _host_arr(e) != n * k):
+            raise ValueError("inconsistent matvec batch shapes")
+        items.append(MatvecBatch(k, n, A.ctypes.data, s.ctypes.data,
+                                 e.ctypes.data if e is not None else None, out.ctypes.data))
+    return (MatvecBatch * len(items))(*items), len(items)
+
+
+def matvec_host_noalloc(batches, stream=0):
+    """tk_matvec_host_noalloc: like matvec_host, staged in the library's static
+    device scratch (NOALLOC_SCRATCH_BYTES); allocates nothing."""
+    arr, n = _host_batches(batches)
+    _check(lib().tk_matvec_host_noalloc(arr, n, int(getattr(stream, "cuda_stream", stream))))
 
 
 def matvec_host(batches):

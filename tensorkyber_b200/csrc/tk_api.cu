@@ -518,6 +518,105 @@ int tk_matvec_host(const tk_matvec_batch* batches, int nbatches) {
   return TK_SUCCESS;
 }
 
+// ---- tk_matvec_host_noalloc: staging in a static device array ----------------
+// The same copy-in / kernels / copy-out sequence as tk_matvec_host, but the
+// staging block is a file-scope device array of TK_NOALLOC_SCRATCH_BYTES
+// (allocated with the module, never by a call) and the work runs on the
+// caller's stream: no cudaMalloc, cudaFree or stream creation on any call.
+// Per device, the first call (with that device current) looks up the array's
+// address with cudaGetSymbolAddress.  Every scratch byte the kernels read is
+// written earlier in the same call (inputs copied in; outputs written by the
+// kernels before they are copied out), so nothing has to start at zero.  One
+// array per device: calls that overlap in time on one device race.
+static __device__ __align__(256) uint8_t g_noalloc_scratch[TK_NOALLOC_SCRATCH_BYTES];
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[kMaxDevices];
+
+int tk_matvec_host_noalloc(const tk_matvec_batch* batches, int nbatches, tk_stream_t stream) {
+  t_err[0] = 0;
+  int nonempty = 0;
+  int rc = validate_matvec(batches, nbatches, true, &nonempty);
+  if (rc || nonempty == 0) return rc;
+  size_t need = 0;
+  for (int b = 0; b < nbatches; b++) {
+    const tk_matvec_batch& B = batches[b];
+    const size_t vb = B.njobs * (size_t)B.k * 512u;
+    need += (vb * (size_t)B.k + vb * (B.e ? 3 : 2) + 255) & ~(size_t)255;
+  }
+  if (need > TK_NOALLOC_SCRATCH_BYTES) {
+    snprintf(t_err, sizeof(t_err),
+             "tk_matvec_host_noalloc: the batch list needs %zu bytes of staging, above the "
+             "%d-byte static scratch",
+             need, TK_NOALLOC_SCRATCH_BYTES);
+    return TK_ERR_TOO_LARGE;
+  }
+  int dev;
+  if ((rc = current_device(&dev))) return rc;
+  DeviceInfo* info;
+  if ((rc = ensure_ready(dev, &info))) return rc;
+  uint8_t* scratch;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p) {
+        set_err("tk_matvec_host_noalloc: cudaGetSymbolAddress of the static scratch", e);
+        return TK_ERR_CUDA;
+      }
+      g_noalloc_ptr[dev] = p;
+    }
+    scratch = (uint8_t*)g_noalloc_ptr[dev];
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  tk_matvec_batch dev_batches[16];
+  if (nbatches > 16) {
+    set_msg("tk_matvec_host_noalloc: at most 16 batches per call");
+    return TK_ERR_INVALID_VALUE;
+  }
+  cudaError_t e = cudaSuccess;
+  size_t off = 0;
+  for (int b = 0; b < nbatches && e == cudaSuccess; b++) {
+    const tk_matvec_batch& B = batches[b];
+    tk_matvec_batch& D = dev_batches[b];
+    D = B;
+    if (B.njobs == 0) continue;
+    const size_t vb = B.njobs * (size_t)B.k * 512u, ab = vb * (size_t)B.k;
+    int16_t* dA = (int16_t*)(scratch + off);
+    int16_t* ds = (int16_t*)(scratch + off + ab);
+    int16_t* de = B.e ? (int16_t*)(scratch + off + ab + vb) : nullptr;
+    int16_t* dout = (int16_t*)(scratch + off + ab + vb * (B.e ? 2 : 1));
+    off += (ab + vb * (B.e ? 3 : 2) + 255) & ~(size_t)255;
+    e = cudaMemcpyAsync(dA, B.A, ab, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ds, B.s, vb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && de) e = cudaMemcpyAsync(de, B.e, vb, cudaMemcpyHostToDevice, st);
+    D.A = dA;
+    D.s = ds;
+    D.e = de;
+    D.out = dout;
+  }
+  if (e == cudaSuccess) {
+    rc = launch_matvec_batches(dev_batches, nbatches, info, st);
+    if (rc) {
+      cudaStreamSynchronize(st);
+      return rc;
+    }
+  }
+  for (int b = 0; b < nbatches && e == cudaSuccess; b++) {
+    const tk_matvec_batch& B = batches[b];
+    if (B.njobs == 0) continue;
+    e = cudaMemcpyAsync(B.out, dev_batches[b].out, B.njobs * (size_t)B.k * 512u,
+                        cudaMemcpyDeviceToHost, st);
+  }
+  const cudaError_t e2 = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = e2;
+  if (e != cudaSuccess) {
+    set_err("tk_matvec_host_noalloc", e);
+    return TK_ERR_CUDA;
+  }
+  return TK_SUCCESS;
+}
+
 int tk_invntt_host(int16_t* polys, size_t npoly) { return run_host(true, polys, npoly); }
 
 int tk_init(int device) {
