@@ -75,6 +75,26 @@ int tk_invntt_oop(const int16_t *in, int16_t *out, size_t npoly, tk_stream_t str
 int tk_ntt_host(int16_t *polys, size_t npoly);
 int tk_invntt_host(int16_t *polys, size_t npoly);
 
+/* ---- small and packed forward inputs ---------------------------------------
+ * Forward NTT of polynomials whose coefficients lie in [-128, 127] (ML-KEM
+ * secrets and noise): stage 1 runs on one data byte per coefficient instead
+ * of two (the reference's single-limb BASIC core,
+ * ntt_bench/ntt_kernels.cuh:406-428).  in and out: device int16 rows, equal
+ * (in place) or disjoint.  A coefficient outside the range sets
+ * TK_FLAG_SMALL_RANGE (tk_device_status) and leaves that output unspecified.
+ * Output as tk_ntt: NTT domain, [0, q). */
+int tk_ntt_small(const int16_t *in, int16_t *out, size_t npoly, tk_stream_t stream);
+/* Forward NTT of packed small polynomials (the reference's TC-PACK input,
+ * ntt_bench/ntt_bench.cu:284-391): bits = 2 (64 bytes per polynomial,
+ * coefficients in [-2, 1]) or 3 (128 bytes, [-4, 3]); coefficient i is the
+ * two's-complement field at bit (i % (8/bits)) * bits of byte i / (8/bits).
+ * packed: device memory, 16-byte aligned, not overlapping out. */
+int tk_ntt_packed(const void *packed, int bits, int16_t *out, size_t npoly, tk_stream_t stream);
+/* Host helper: packs npoly int16 polynomials into that format (packed must
+ * hold npoly * 32 * bits bytes for bits = 2, npoly * 128 for bits = 3).
+ * TK_ERR_INVALID_VALUE if a coefficient does not fit in `bits` bits. */
+int tk_pack_small(const int16_t *polys, size_t npoly, int bits, void *packed);
+
 /* ---- matrix-vector jobs (ML-KEM shape) ----------------------------------
  * For every job and i < k:
  *     out_i = invntt( sum_j basemul(A_ij, ntt(s_j)) ) + e_i       (mod q)
@@ -188,7 +208,11 @@ long long tk_get_option(int option);
 int tk_init(int device);
 
 /* Reads and clears the kernel-side error flags of a device (bit 0: forward,
- * bit 1: inverse kernel gave up on a bounded wait).  Synchronous. */
+ * bit 1: inverse kernel gave up on a bounded wait; bit 2: tk_ntt_small saw a
+ * coefficient outside [-128, 127]).  Synchronous. */
+#define TK_FLAG_FORWARD_TIMEOUT 1u
+#define TK_FLAG_INVERSE_TIMEOUT 2u
+#define TK_FLAG_SMALL_RANGE 4u
 int tk_device_status(int device, unsigned *flags);
 
 /* ---- kernel variants ------------------------------------------------------

@@ -68,6 +68,9 @@ class Oracle:
         L.tko_basemul.argtypes = [_I16P, _I16P, _I16P, ctypes.c_int16]
         L.tko_poly_basemul.argtypes = [_I16P, _I16P, _I16P]
         L.tko_matvec_job.argtypes = [ctypes.c_int, _I16P, _I16P, _I16P, _I16P]
+        L.tko_pack_small.argtypes = [ctypes.c_int, _I16P, ctypes.c_void_p]
+        L.tko_pack_small.restype = ctypes.c_size_t
+        L.tko_unpack_small.argtypes = [ctypes.c_int, ctypes.c_void_p, _I16P]
         L.tko_montgomery_reduce.argtypes = [ctypes.c_int32]
         L.tko_montgomery_reduce.restype = ctypes.c_int16
         L.tko_barrett_reduce.argtypes = [ctypes.c_int16]
@@ -107,6 +110,22 @@ class Oracle:
         e = np.ascontiguousarray(e, dtype=np.int16).reshape(k, N)
         out = np.zeros((k, N), dtype=np.int16)
         self.lib.tko_matvec_job(k, _ptr(A), _ptr(s), _ptr(e), _ptr(out))
+        return out
+
+    def pack_small(self, bits: int, polys: np.ndarray) -> np.ndarray:
+        """(npoly, 256) small int16 -> (npoly, 256*bits/8 rounded) packed bytes."""
+        p = np.ascontiguousarray(polys, dtype=np.int16).reshape(-1, 256)
+        per = 8 // bits
+        out = np.zeros((p.shape[0], (256 + per - 1) // per), dtype=np.uint8)
+        for i in range(p.shape[0]):
+            self.lib.tko_pack_small(bits, _ptr(p[i]), out[i].ctypes.data)
+        return out
+
+    def unpack_small(self, bits: int, packed: np.ndarray) -> np.ndarray:
+        pk = np.ascontiguousarray(packed, dtype=np.uint8)
+        out = np.zeros((pk.shape[0], 256), dtype=np.int16)
+        for i in range(pk.shape[0]):
+            self.lib.tko_unpack_small(bits, pk[i].ctypes.data, _ptr(out[i]))
         return out
 
     def fn(self, name: str) -> int:

@@ -276,3 +276,22 @@ double tko_split_roundtrip(tko_poly_fn fwd, tko_poly_fn inv, int16_t *polys, siz
   free(tid);
   return dt;
 }
+
+/* ntt_bench/ntt_bench.cu:744-752: per = 8/bits fields per byte, low bits first. */
+size_t tko_pack_small(int bits, const int16_t poly[256], uint8_t *packed) {
+  const int per = 8 / bits;
+  const size_t nbytes = (256 + per - 1) / per;
+  memset(packed, 0, nbytes);
+  for (int i = 0; i < 256; i++)
+    packed[i / per] |= (uint8_t)((poly[i] & ((1 << bits) - 1)) << ((i % per) * bits));
+  return nbytes;
+}
+
+/* ntt_bench/ntt_bench.cu:317-340: the field, sign-extended from `bits` bits. */
+void tko_unpack_small(int bits, const uint8_t *packed, int16_t poly[256]) {
+  const int per = 8 / bits;
+  for (int i = 0; i < 256; i++) {
+    const int code = (packed[i / per] >> ((i % per) * bits)) & ((1 << bits) - 1);
+    poly[i] = (int16_t)(code >= (1 << (bits - 1)) ? code - (1 << bits) : code);
+  }
+}

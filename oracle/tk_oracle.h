@@ -80,6 +80,15 @@ double tko_time_roundtrip(tko_poly_fn fwd, tko_poly_fn inv, const int16_t *src,
                           size_t npoly, int threads, double min_seconds,
                           uint64_t *polys_done);
 
+/* Packed small-coefficient polynomials (the TC-PACK input format): `bits`-bit
+ * two's-complement fields, 8/bits coefficients per byte, coefficient i in
+ * byte i/(8/bits) at bit (i % (8/bits))*bits.  tko_pack_small restates the
+ * reference harness's pack_small (ntt_bench/ntt_bench.cu:744-752) and returns
+ * the bytes per polynomial; tko_unpack_small restates the kernel's unpacking
+ * with sign extension (ntt_bench/ntt_bench.cu:317-340).  bits is 2 or 3. */
+size_t tko_pack_small(int bits, const int16_t poly[256], uint8_t *packed);
+void tko_unpack_small(int bits, const uint8_t *packed, int16_t poly[256]);
+
 /* One pass: polys (npoly, in place) is split into `threads` contiguous
  * chunks and each thread applies fwd() then inv() to every poly of its chunk.
  * Returns the wall time in seconds (negative on failure). */

@@ -123,6 +123,13 @@ def lib() -> ctypes.CDLL:
     L.tk_autotune.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.c_char_p]
     L.tk_autotune.restype = ctypes.c_int
     L.tk_autotune_reset.restype = ctypes.c_int
+    L.tk_ntt_small.argtypes = [p16, p16, ctypes.c_size_t, ctypes.c_void_p]
+    L.tk_ntt_small.restype = ctypes.c_int
+    L.tk_ntt_packed.argtypes = [ctypes.c_void_p, ctypes.c_int, p16, ctypes.c_size_t,
+                                ctypes.c_void_p]
+    L.tk_ntt_packed.restype = ctypes.c_int
+    L.tk_pack_small.argtypes = [p16, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p]
+    L.tk_pack_small.restype = ctypes.c_int
     L.tk_matvec.argtypes = [ctypes.POINTER(MatvecBatch), ctypes.c_int, ctypes.c_void_p]
     L.tk_matvec.restype = ctypes.c_int
     L.tk_matvec_host.argtypes = [ctypes.POINTER(MatvecBatch), ctypes.c_int]
@@ -233,6 +240,48 @@ def invntt_host(a: np.ndarray) -> np.ndarray:
     """Inverse NTT of host polynomials in place (synchronous, through the GPU)."""
     _check(lib().tk_invntt_host(a.ctypes.data, _host_arr(a)))
     return a
+
+
+FLAG_FORWARD_TIMEOUT, FLAG_INVERSE_TIMEOUT, FLAG_SMALL_RANGE = 1, 2, 4
+
+
+def ntt_small(polys, out=None, stream=None):
+    """Forward NTT of CUDA int16 polynomials with coefficients in [-128, 127]
+    (single-limb stage 1).  Out-of-range inputs set FLAG_SMALL_RANGE."""
+    n = _check_tensor(polys)
+    if out is None:
+        out = polys
+    elif _check_tensor(out) != n:
+        raise ValueError("out must hold as many polynomials as polys")
+    _check(lib().tk_ntt_small(polys.data_ptr(), out.data_ptr(), n, _stream_ptr(stream)))
+    return out
+
+
+def ntt_packed(packed, bits, out=None, stream=None):
+    """Forward NTT of packed small polynomials: packed is a CUDA uint8 tensor
+    of (npoly, 256 * bits / 8 rounded to 64 or 128) bytes; returns int16
+    (npoly, 256) NTT-domain polynomials in [0, q)."""
+    import torch
+    row = 64 if bits == 2 else 128
+    if not isinstance(packed, torch.Tensor) or packed.dtype != torch.uint8 or not packed.is_cuda \
+            or not packed.is_contiguous() or packed.numel() % row:
+        raise TypeError(f"expected a contiguous CUDA uint8 tensor of {row}-byte rows")
+    n = packed.numel() // row
+    if out is None:
+        out = torch.empty((n, N), dtype=torch.int16, device=packed.device)
+    elif _check_tensor(out) != n:
+        raise ValueError("out must hold one polynomial per packed row")
+    _check(lib().tk_ntt_packed(packed.data_ptr(), bits, out.data_ptr(), n, _stream_ptr(stream)))
+    return out
+
+
+def pack_small(polys: np.ndarray, bits: int) -> np.ndarray:
+    """Host packing of int16 polynomials into the tk_ntt_packed format."""
+    n = _host_arr(polys)
+    row = 64 if bits == 2 else 128
+    out = np.zeros((n, row), dtype=np.uint8)
+    _check(lib().tk_pack_small(polys.ctypes.data, n, bits, out.ctypes.data))
+    return out
 
 
 def matvec(batches, stream=None):

@@ -318,6 +318,93 @@ int tk_invntt_oop(const int16_t* in, int16_t* out, size_t npoly, tk_stream_t str
 }
 int tk_ntt_host(int16_t* polys, size_t npoly) { return run_host(false, polys, npoly); }
 
+// Forward transform of an input form (1: small int16, 2/3: packed) on device
+// buffers; in_bytes per polynomial of the input.
+static int run_form(int form, const void* in, int16_t* out, size_t npoly, size_t in_bytes,
+                    cudaStream_t st) {
+  t_err[0] = 0;
+  if (npoly == 0) return TK_SUCCESS;
+  if (!in || !out) {
+    set_msg("NULL buffer pointer");
+    return TK_ERR_INVALID_VALUE;
+  }
+  if (npoly > TK_MAX_POLYS) {
+    set_msg("npoly above TK_MAX_POLYS");
+    return TK_ERR_TOO_LARGE;
+  }
+  if (((uintptr_t)in & 15u) || ((uintptr_t)out & 15u)) {
+    set_msg("buffers must be 16-byte aligned");
+    return TK_ERR_MISALIGNED;
+  }
+  const uintptr_t a = (uintptr_t)in, b = (uintptr_t)out;
+  const uintptr_t na = (uintptr_t)npoly * in_bytes, nb = (uintptr_t)npoly * 512u;
+  const bool same = form == 1 && a == b;
+  if (!same && a < b + nb && b < a + na) {
+    set_msg(form == 1 ? "input and output overlap without being identical"
+                      : "packed input overlaps the output");
+    return TK_ERR_INVALID_VALUE;
+  }
+  int dev;
+  int rc = current_device(&dev);
+  if (rc) return rc;
+  DeviceInfo* info;
+  if ((rc = ensure_ready(dev, &info))) return rc;
+  if ((rc = check_device_ptr(in))) return rc;
+  if (!same && (rc = check_device_ptr(out))) return rc;
+  const cudaError_t e = tk::launch_fwd_form(form, in, out, (long long)npoly, *info, st);
+  if (e != cudaSuccess) {
+    set_launch_err(e);
+    return TK_ERR_CUDA;
+  }
+  return TK_SUCCESS;
+}
+
+int tk_ntt_small(const int16_t* in, int16_t* out, size_t npoly, tk_stream_t stream) {
+  return run_form(1, in, out, npoly, 512, (cudaStream_t)stream);
+}
+
+int tk_ntt_packed(const void* packed, int bits, int16_t* out, size_t npoly, tk_stream_t stream) {
+  if (bits != 2 && bits != 3) {
+    t_err[0] = 0;
+    set_msg("tk_ntt_packed: bits must be 2 or 3");
+    return TK_ERR_INVALID_VALUE;
+  }
+  return run_form(bits, packed, out, npoly, bits == 2 ? 64 : 128, (cudaStream_t)stream);
+}
+
+// Host-side packing (the format of tk_ntt_packed); a plain data conversion,
+// not a transform.
+int tk_pack_small(const int16_t* polys, size_t npoly, int bits, void* packed) {
+  t_err[0] = 0;
+  if (bits != 2 && bits != 3) {
+    set_msg("tk_pack_small: bits must be 2 or 3");
+    return TK_ERR_INVALID_VALUE;
+  }
+  if (npoly == 0) return TK_SUCCESS;
+  if (!polys || !packed) {
+    set_msg("tk_pack_small: NULL pointer");
+    return TK_ERR_INVALID_VALUE;
+  }
+  const int per = 8 / bits, lo = -(1 << (bits - 1)), hi = (1 << (bits - 1)) - 1;
+  const size_t row = 256 / per;
+  uint8_t* dst = (uint8_t*)packed;
+  for (size_t p = 0; p < npoly; p++) {
+    const int16_t* x = polys + p * 256;
+    uint8_t* d = dst + p * row;
+    memset(d, 0, row);
+    for (int i = 0; i < 256; i++) {
+      if (x[i] < lo || x[i] > hi) {
+        snprintf(t_err, sizeof(t_err),
+                 "tk_pack_small: polynomial %zu coefficient %d = %d outside [%d, %d]", p, i,
+                 (int)x[i], lo, hi);
+        return TK_ERR_INVALID_VALUE;
+      }
+      d[i / per] |= (uint8_t)((x[i] & ((1 << bits) - 1)) << ((i % per) * bits));
+    }
+  }
+  return TK_SUCCESS;
+}
+
 static bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
   const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
   return x < y + nb && y < x + na;

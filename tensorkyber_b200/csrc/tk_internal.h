@@ -14,11 +14,16 @@ constexpr int kNumMmaVariants = 3;
 // Largest batch one kernel launch covers (TMA coordinates are signed 32-bit).
 constexpr long long kMaxLaunchPolys = 1ll << 30;
 
+// Forward input forms besides int16: 1 = int16 with coefficients in
+// [-128, 127], 2 / 3 = packed 2- / 3-bit fields (single-limb stage 1).
+constexpr int kNumInputForms = 3;
+
 struct DeviceInfo {
   int device = -1;
   int num_sms = 0;
   int cc_major = 0, cc_minor = 0;
   int mma_ctas_per_sm[2][kNumMmaVariants] = {{1, 1, 1}, {1, 1, 1}};  // [inverse][variant]
+  int form_ctas_per_sm[kNumInputForms] = {1, 1, 1};  // forward input forms 1..3
   size_t total_mem = 0;
 };
 
@@ -104,6 +109,13 @@ int api_device_info(int device, DeviceInfo** info);
 // allocation (a copy that runs from one page-locked allocation into the next
 // is not valid).  Needs the device's context current on the calling thread.
 bool host_span_one_copy(const void* p, size_t bytes);
+
+// Forward transform of npoly polynomials given in input form `form` (1..3):
+// src holds int16 rows (form 1; src == dst for in place) or packed rows of
+// 64 / 128 bytes (forms 2 / 3); dst gets int16 NTT-domain rows in [0, q).
+// Form 1 sets status bit 2 when an input lies outside [-128, 127].
+cudaError_t launch_fwd_form(int form, const void* src, int16_t* dst, long long npoly,
+                            const DeviceInfo& info, cudaStream_t stream);
 
 // Kernel-side error flags (bounded waits that gave up), read and reset.
 cudaError_t read_and_clear_status(unsigned* flags);

@@ -30,9 +30,9 @@
 //            order), CTA barrier, stage B (Minv) by polynomial (as forward
 //            stage 1, output centred), then each warp stores its own polys
 //   store    tensor TMA smem -> global; at the top of the next iteration the
-//            slot is refilled (two tiles ahead) once that store was read out
-//            of smem (wait_group.read), so two loads stay in flight while a
-//            tile is computed
+//            slot is refilled (S-1 tiles ahead, S = slots) once that store was
+//            read out of smem (wait_group.read), so S-1 loads stay in flight
+//            while a tile is computed
 //
 // Reference counterparts: the in-place batch kernels k_ntt_2tc_tc_cc /
 // k_invntt_2tc_tc_cc / k_ntt_tc_cc_cp / k_invntt_tc_cc_cp
@@ -59,12 +59,24 @@ __device__ FwdFrags g_fwd;
 __device__ InvFrags g_inv;
 __device__ unsigned int g_status;
 
-template <int W, int S>
+// Forward input forms: int16 polynomials (any value), int16 polynomials with
+// coefficients in [-128, 127] (single-limb stage 1), and packed 2- or 3-bit
+// fields (TC-PACK format, single-limb stage 1).
+enum InForm { kInInt16 = 0, kInSmall = 1, kInPack2 = 2, kInPack3 = 3 };
+template <int kIn>
+constexpr int packed_row_bytes() {
+  return kIn == kInPack2 ? 64 : kIn == kInPack3 ? 128 : 0;
+}
+
+template <int W, int S, int kIn = kInInt16>
 struct Cfg {
   static constexpr int kWarps = W;
   static constexpr int kThreads = 32 * W;
   static constexpr int kTile = 8 * W;                 // polynomials per tile
-  static constexpr int kSlotBytes = kTile * kRowBytes;
+  // a slot: kTile padded rows, then (packed forms) the tile's packed input
+  static constexpr int kPackBytes = packed_row_bytes<kIn>();
+  static constexpr int kRowsBytes = kTile * kRowBytes;
+  static constexpr int kSlotBytes = kTile * (kRowBytes + kPackBytes);
   static constexpr int kSlots = S;
   static constexpr int kSmem = S * kSlotBytes + 16 * S;  // slots + mbarriers
   static constexpr int kBlocksPerWarp = 16 / W;       // block-wise stages
@@ -167,12 +179,70 @@ __device__ __forceinline__ void poly_stage(uint32_t mine, uint8_t* minep, uint32
   }
 }
 
+// Forward stage 1 of this warp's 8 polynomials in single-limb form.  kInSmall:
+// operands from the int16 rows (ldmatrix.trans as poly_stage, low bytes);
+// packed forms: from the tile's packed rows (packp: this warp's 8 rows of
+// kPackBytes), which lane (t = lane%4, n = lane/4) reads as the words of blocks
+// m = 2t, 2t+1, 8+2t, 9+2t.
+template <int kIn>
+__device__ __forceinline__ void poly_stage_small(uint32_t mine, uint8_t* minep, uint32_t ldt_off,
+                                                 const uint8_t* packp, const uint32_t (&ab)[2][2],
+                                                 int32_t cb_lo, int32_t cb_hi, uint32_t w_even,
+                                                 uint32_t w_odd, int lane, uint32_t* bad) {
+  const uint32_t t = lane & 3, n = lane >> 2;
+  if (kIn == kInSmall) {
+    uint32_t b[4];
+    ldsm_x4_t(mine + ldt_off, b[0], b[1], b[2], b[3]);
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+      uint32_t nx[4] = {0, 0, 0, 0};
+      if (p < 7) ldsm_x4_t(mine + (p + 1) * kRowBytes + ldt_off, nx[0], nx[1], nx[2], nx[3]);
+      const uint32_t bt0 = small_operand(b[0], b[1], bad);
+      const uint32_t bt1 = small_operand(b[2], b[3], bad);
+      stage_m_small(ab, cb_lo, cb_hi, bt0, bt1, minep + p * kRowBytes, w_even, w_odd);
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = nx[j];
+    }
+  } else if (kIn == kInPack2) {
+    // 4 bytes per block m (coefficients 16m .. 16m+15); coefficient c of the
+    // block is byte c/4, bits 2(c%4): n-tile 0 byte n/4, n-tile 1 byte 2 + n/4
+    const uint32_t k0 = n >> 2, k1 = k0 + 2;
+    const uint32_t sel0 = k0 | ((k0 + 4) << 4), sel1 = k1 | ((k1 + 4) << 4);
+    const uint32_t shift = 2 * (n & 3);
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+      const uint8_t* pk = packp + p * 64;
+      const uint2 v01 = *(const uint2*)(pk + 8 * t);       // m = 2t, 2t+1
+      const uint2 v23 = *(const uint2*)(pk + 32 + 8 * t);  // m = 8+2t, 9+2t
+      const uint32_t bt0 = packed_operand<2>(v01.x, v01.y, v23.x, v23.y, sel0, shift);
+      const uint32_t bt1 = packed_operand<2>(v01.x, v01.y, v23.x, v23.y, sel1, shift);
+      stage_m_small(ab, cb_lo, cb_hi, bt0, bt1, minep + p * kRowBytes, w_even, w_odd);
+    }
+  } else {
+    // 8 bytes per block m; coefficient c is byte c/2, bits 3(c%2): n-tile 0
+    // uses each block's first word (byte n/2), n-tile 1 its second word
+    const uint32_t k = n >> 1;
+    const uint32_t sel = k | ((k + 4) << 4);
+    const uint32_t shift = 3 * (n & 1);
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+      const uint8_t* pk = packp + p * 128;
+      const uint4 v01 = *(const uint4*)(pk + 16 * t);       // m = 2t, 2t+1
+      const uint4 v23 = *(const uint4*)(pk + 64 + 16 * t);  // m = 8+2t, 9+2t
+      const uint32_t bt0 = packed_operand<3>(v01.x, v01.z, v23.x, v23.z, sel, shift);
+      const uint32_t bt1 = packed_operand<3>(v01.y, v01.w, v23.y, v23.w, sel, shift);
+      stage_m_small(ab, cb_lo, cb_hi, bt0, bt1, minep + p * kRowBytes, w_even, w_odd);
+    }
+  }
+}
+
 // ------------------------------------------------------------ the kernel ---
-template <bool kInverse, int W, int S>
-__global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
+template <bool kInverse, int W, int S, int kIn = kInInt16>
+__global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
     k_ntt_mma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_out,
               int npoly, const uint32_t* __restrict__ addend) {
-  using C = Cfg<W, S>;
+  static_assert(!kInverse || kIn == kInInt16, "input forms are forward only");
+  using C = Cfg<W, S, kIn>;
   extern __shared__ __align__(128) uint8_t smem[];
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -197,6 +267,17 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
     for (int j = 0; j < 4; j++) am[g][j] = kInverse ? g_inv.sb[g][lane][j] : g_fwd.s1[g][lane][j];
   cm_lo = kInverse ? 1664 : g_fwd.c1[lane][0];
   cm_hi = kInverse ? 1664 : g_fwd.c1[lane][1];
+  uint32_t ab[2][2] = {{0, 0}, {0, 0}};  // single-limb stage 1 (input forms)
+  int32_t cb_lo = 0, cb_hi = 0;
+  if (kIn != kInInt16) {
+#pragma unroll
+    for (int g = 0; g < 2; g++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) ab[g][j] = g_fwd.s1b[g][lane][j];
+    cb_lo = g_fwd.c1b[lane][0];
+    cb_hi = g_fwd.c1b[lane][1];
+  }
+  uint32_t bad = 0;  // kInSmall: inputs outside [-128, 127] seen
 #pragma unroll
   for (int p = 0; p < C::kPairsPerWarp; p++)
 #pragma unroll
@@ -246,9 +327,15 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
     const int unit = u_begin + k * W + warp;
     const uint32_t bar = bar0 + 8 * slot_i;
     if (unit < u_end) {
-      mbar_expect_tx(bar, kWarpBoxBytes);
-      tma_load_2d(smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes, &tm_in, 0, 8 * unit,
-                  bar);
+      if (C::kPackBytes) {  // the packed rows, after the tile's padded rows
+        mbar_expect_tx(bar, 8 * C::kPackBytes);
+        tma_load_2d(smem0 + slot_i * C::kSlotBytes + C::kRowsBytes + warp * 8 * C::kPackBytes,
+                    &tm_in, 0, 8 * unit, bar);
+      } else {
+        mbar_expect_tx(bar, kWarpBoxBytes);
+        tma_load_2d(smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes, &tm_in, 0, 8 * unit,
+                    bar);
+      }
     } else {
       mbar_expect_tx(bar, 0);  // arrive only
     }
@@ -261,8 +348,10 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
     bulk_commit();
   };
 
-  issue_load(0, 0);
-  if (nmine > 1) issue_load(1, 1);
+  // prologue: tiles 0 .. S-2 into slots 0 .. S-2
+#pragma unroll
+  for (int t = 0; t < C::kSlots - 1; t++)
+    if (t < nmine) issue_load(t, t);
 
   int slot_i = 0;
   uint32_t phase = 0;
@@ -274,22 +363,32 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
       if (tid == 0) atomicOr(&g_status, kInverse ? 2u : 1u);
       break;
     }
-    if (k + 2 < nmine) {
-      // refill early: the slot of tile k+2 last held tile k-1, whose compute
-      // finished before the barrier above; its store (issued by this lane,
-      // for this warp's rows) must have been read out of smem.
+    if (k + C::kSlots - 1 < nmine) {
+      // refill early: tile k+S-1 goes to the slot that held tile k-1, whose
+      // compute finished before the barrier above; its store (issued by this
+      // lane, for this warp's rows) must have been read out of smem.
       if (lane == 0) bulk_wait_read<0>();
-      int s2 = slot_i + 2;
+      int s2 = slot_i + C::kSlots - 1;
       if (s2 >= C::kSlots) s2 -= C::kSlots;
-      issue_load(k + 2, s2);
+      issue_load(k + C::kSlots - 1, s2);
     }
     // own polynomials of this warp: rows 8w .. 8w+7
     const uint32_t mine = slot + 8 * warp * kRowBytes;
     uint8_t* minep = slotp + 8 * warp * kRowBytes;
 
     if (!kInverse) {
-      poly_stage<false>(mine, minep, ldt_off, am, cm_lo, cm_hi, w_even, w_odd, 0, nullptr, 0, 0,
-                        0);
+      if (kIn == kInInt16)
+        poly_stage<false>(mine, minep, ldt_off, am, cm_lo, cm_hi, w_even, w_odd, 0, nullptr, 0, 0,
+                          0);
+      else {
+        // a warp without a unit in this tile computes on stale rows (its
+        // result is never stored): only live rows count for the range check
+        uint32_t tile_bad = 0;
+        poly_stage_small<kIn>(mine, minep, ldt_off,
+                              slotp + C::kRowsBytes + warp * 8 * C::kPackBytes, ab, cb_lo, cb_hi,
+                              w_even, w_odd, lane, &tile_bad);
+        if (u_begin + k * W + warp < u_end) bad |= tile_bad;
+      }
       cta_sync_named();
       block_stage<false, W>(slot, slotp, blk0, ldc_off, stc_off, ac, cc);
       fence_proxy_async_smem();
@@ -310,6 +409,7 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S>::kMinBlocks)
     }
   }
   if (lane == 0) bulk_wait_all();
+  if (kIn == kInSmall && __any_sync(0xffffffffu, bad != 0) && lane == 0) atomicOr(&g_status, 4u);
 }
 
 // ------------------------------------------------------------ host side ----
@@ -332,6 +432,18 @@ static const Variant kVariants[2][kNumMmaVariants] = {
     {make_variant<false, 4, 3>(), make_variant<false, 8, 3>(), make_variant<false, 4, 2>()},
     {make_variant<true, 4, 3>(), make_variant<true, 8, 3>(), make_variant<true, 4, 2>()},
 };
+
+// Forward kernels for the small / packed input forms: 4 warps; 3 slots for
+// int16 rows, 2 for packed rows (their loads are 8x smaller, and the smaller
+// slots let 5 CTAs share an SM instead of 3).
+template <int kIn, int S>
+constexpr Variant make_form_variant() {
+  using C = Cfg<4, S, kIn>;
+  return Variant{k_ntt_mma<false, 4, S, kIn>, C::kThreads, C::kSmem, C::kTile};
+}
+static const Variant kFormVariants[kNumInputForms] = {make_form_variant<kInSmall, 3>(),
+                                                      make_form_variant<kInPack2, 2>(),
+                                                      make_form_variant<kInPack3, 2>()};
 
 static thread_local int g_last_encode_result = 0;
 
@@ -360,6 +472,25 @@ static bool encode_batch_map(CUtensorMap* map, const int16_t* base, int npoly) {
   const cuuint64_t dims[2] = {128, (cuuint64_t)npoly};
   const cuuint64_t strides[1] = {512};
   const cuuint32_t box[2] = {kRowBytes / 4, 8};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r =
+      enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, (void*)base, dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  g_last_encode_result = (int)r;
+  return r == CUDA_SUCCESS;
+}
+
+// A packed batch as a [npoly][row_bytes / 4] uint32 tensor, boxes of 8 rows.
+static bool encode_packed_map(CUtensorMap* map, const void* base, int npoly, int row_bytes) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+  if (!enc) {
+    g_last_encode_result = -1;
+    return false;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)(row_bytes / 4), (cuuint64_t)npoly};
+  const cuuint64_t strides[1] = {(cuuint64_t)row_bytes};
+  const cuuint32_t box[2] = {(cuuint32_t)(row_bytes / 4), 8};
   const cuuint32_t estr[2] = {1, 1};
   const CUresult r =
       enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, (void*)base, dims, strides, box, estr,
@@ -401,7 +532,60 @@ bool mma_init_device(DeviceInfo* info) {
         return false;
       info->mma_ctas_per_sm[inv][v] = per_sm > 0 ? per_sm : 1;
     }
+  for (int f = 0; f < kNumInputForms; f++) {
+    const Variant& V = kFormVariants[f];
+    if (cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, V.smem) !=
+        cudaSuccess)
+      return false;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, V.fn, V.threads, V.smem) !=
+        cudaSuccess)
+      return false;
+    info->form_ctas_per_sm[f] = per_sm > 0 ? per_sm : 1;
+  }
   return true;
+}
+
+static cudaError_t launch_variant(const Variant& V, long long cap, const CUtensorMap& m_in,
+                                  const CUtensorMap& m_out, int n, const uint32_t* add,
+                                  cudaStream_t stream) {
+  long long ctas = (n + V.tile - 1) / V.tile;
+  if (ctas > cap) ctas = cap;
+  if (ctas < 1) ctas = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)ctas);
+  cfg.blockDim = dim3((unsigned)V.threads);
+  cfg.dynamicSmemBytes = (size_t)V.smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, V.fn, m_in, m_out, n, add);
+}
+
+cudaError_t launch_fwd_form(int form, const void* src, int16_t* dst, long long npoly,
+                            const DeviceInfo& info, cudaStream_t stream) {
+  if (form < 1 || form > kNumInputForms) return cudaErrorInvalidValue;
+  const Variant& V = kFormVariants[form - 1];
+  const long long cap = (long long)info.num_sms * info.form_ctas_per_sm[form - 1];
+  const int row_bytes = form == kInPack2 ? 64 : form == kInPack3 ? 128 : 512;
+  for (long long done = 0; done < npoly; done += kMaxLaunchPolys) {
+    const int n = (int)((npoly - done) < kMaxLaunchPolys ? (npoly - done) : kMaxLaunchPolys);
+    const uint8_t* in = (const uint8_t*)src + done * row_bytes;
+    CUtensorMap m_in, m_out;
+    const bool ok_in = form == kInSmall ? encode_batch_map(&m_in, (const int16_t*)in, n)
+                                        : encode_packed_map(&m_in, in, n, row_bytes);
+    if (!ok_in) return cudaErrorInvalidResourceHandle;
+    if ((const void*)in == (const void*)(dst + done * 256))
+      m_out = m_in;
+    else if (!encode_batch_map(&m_out, dst + done * 256, n))
+      return cudaErrorInvalidResourceHandle;
+    const cudaError_t e = launch_variant(V, cap, m_in, m_out, n, nullptr, stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* dst,
@@ -419,21 +603,8 @@ cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* d
       m_out = m_in;
     else if (!encode_batch_map(&m_out, dst + done * 256, n))
       return cudaErrorInvalidResourceHandle;
-    long long ctas = (n + V.tile - 1) / V.tile;
-    if (ctas > cap) ctas = cap;
-    if (ctas < 1) ctas = 1;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)ctas);
-    cfg.blockDim = dim3((unsigned)V.threads);
-    cfg.dynamicSmemBytes = (size_t)V.smem;
-    cfg.stream = stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
     const uint32_t* add = addend ? (const uint32_t*)(addend + done * 256) : nullptr;
-    const cudaError_t e = cudaLaunchKernelEx(&cfg, V.fn, m_in, m_out, n, add);
+    const cudaError_t e = launch_variant(V, cap, m_in, m_out, n, add, stream);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

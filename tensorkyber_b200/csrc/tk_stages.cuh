@@ -61,6 +61,61 @@ __device__ __forceinline__ void stage_m(const uint32_t (&a)[2][4], int32_t c_lo,
   }
 }
 
+// Forward stage 1 in single-limb form, for inputs in [-128, 127]: one data
+// byte per coefficient (x + 128) instead of two, so half the MMA work of
+// stage_m.  bt0 / bt1: the m16n8k16 B operands of n-tiles 0 and 1 (c = lane/4
+// and 8 + lane/4), byte j of lane t = lane%4 holding block
+// m = {2t, 2t+1, 8+2t, 9+2t}[j] -- the order of the low bytes in stage_m's
+// k32 fragments, which FwdFrags::s1b's column order follows.  Output as
+// stage_m<false>: lazy Barrett, parity-split rows.
+__device__ __forceinline__ void stage_m_small(const uint32_t (&a)[2][2], int32_t c_lo,
+                                              int32_t c_hi, uint32_t bt0, uint32_t bt1,
+                                              uint8_t* row, uint32_t w_even, uint32_t w_odd) {
+  const int32_t cinit[4] = {c_lo, c_lo, c_hi, c_hi};
+  const int32_t zero[4] = {0, 0, 0, 0};
+  int32_t lo0[4], hi0[4], lo1[4], hi1[4];
+  mma_k16(lo0, a[0], bt0, cinit);
+  mma_k16(hi0, a[1], bt0, zero);
+  mma_k16(lo1, a[0], bt1, cinit);
+  mma_k16(hi1, a[1], bt1, zero);
+  uint32_t y0[4], y1[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    y0[e] = red_lazy((uint32_t)lo0[e] + ((uint32_t)hi0[e] << 7));
+    y1[e] = red_lazy((uint32_t)lo1[e] + ((uint32_t)hi1[e] << 7));
+  }
+  *(uint32_t*)(row + w_even) = pack2(y0[0], y1[0]);
+  *(uint32_t*)(row + w_odd) = pack2(y0[1], y1[1]);
+  *(uint32_t*)(row + w_even + 256) = pack2(y0[2], y1[2]);
+  *(uint32_t*)(row + w_odd + 256) = pack2(y0[3], y1[3]);
+}
+
+// The single-limb B operands from stage_m's two k32 fragment registers of one
+// n-tile (int16 inputs): low bytes, biased to x + 128.  *bad collects bits
+// where a high byte is not the sign extension of its low byte (input outside
+// [-128, 127]).
+__device__ __forceinline__ uint32_t small_operand(uint32_t b0, uint32_t b1, uint32_t* bad) {
+  const uint32_t lo = __byte_perm(b0, b1, 0x6420);
+  const uint32_t hi = __byte_perm(b0, b1, 0x7531);
+  *bad |= hi ^ (((lo >> 7) & 0x01010101u) * 0xffu);
+  return lo ^ 0x80808080u;
+}
+
+// The single-limb B operand of one n-tile from packed fields: w0..w3 hold
+// the packed bytes of blocks m = 2t, 2t+1, 8+2t, 9+2t; byte `sel` (a
+// __byte_perm selector picking byte k of the first and second word) of each
+// holds the field at bit `shift`.  Fields are kBits-bit two's complement; the
+// result byte is value + 128 = (field ^ sign bit) + 128 - 2^(kBits-1).
+template <int kBits>
+__device__ __forceinline__ uint32_t packed_operand(uint32_t w0, uint32_t w1, uint32_t w2,
+                                                   uint32_t w3, uint32_t sel, uint32_t shift) {
+  constexpr uint32_t kMask = ((1u << kBits) - 1u) * 0x01010101u;
+  constexpr uint32_t kSign = (1u << (kBits - 1)) * 0x01010101u;
+  constexpr uint32_t kOff = (128u - (1u << (kBits - 1))) * 0x01010101u;
+  const uint32_t g = __byte_perm(__byte_perm(w0, w1, sel), __byte_perm(w2, w3, sel), 0x5410);
+  return (((g >> shift) & kMask) ^ kSign) + kOff;
+}
+
 // Block-wise stage (forward stage 2 / inverse stage A) for blocks I, I+1 of 8
 // polynomials.  r[0..3]: B operands (even I, odd I, even I+1, odd I+1).
 // Output: natural order, polynomials 2q and 2q+1 of the n-tile.

@@ -155,6 +155,24 @@ void build_fwd_frags(const Matrices& M, FwdFrags* F) {
             return limb(byte_weighted(M.m2[b][co][c], k & 1), r >> 3);
           },
           F->s2[b][s]);
+  // single-limb stage 1: two accumulator groups (lo / hi limb), rows 0..15
+  // on the two A register halves of m16n8k16
+  for (int g = 0; g < 2; g++)
+    pack_a_k16([&](int i, int k) { return limb(M.m1[i][basic_k_block(k)], g); }, F->s1b[g]);
+  for (int i = 0; i < 16; i++) {
+    int64_t rs = 0;
+    for (int m = 0; m < 16; m++) rs += M.m1[i][m];
+    corr[i] = (int32_t)modq(-128 * rs);
+  }
+  for (int lane = 0; lane < 32; lane++) {
+    F->c1b[lane][0] = corr[lane >> 2];
+    F->c1b[lane][1] = corr[(lane >> 2) + 8];
+  }
+}
+
+int basic_k_block(int k) {
+  const int t = k >> 2, j = k & 3;
+  return j < 2 ? 2 * t + j : 8 + 2 * t + (j - 2);
 }
 
 void build_inv_frags(const Matrices& M, InvFrags* F) {

@@ -58,10 +58,18 @@ constexpr uint32_t kBias10qPacked = 0x020A020Au;
 // Forward stage 2: per block b and parity s, A = 16x16 s8 (m16n8k16):
 // rows r<8 -> group 0, r>=8 -> group 1, output c' = 2*(r&7) + s; K k = 2*slot
 // + byte, slot j holds c = 2*e(j) + s with e(j) = (j>>1) + 4*(j&1).
+// Forward stage 1, single-limb form (inputs in [-128, 127], one byte each):
+// A = 16x16 s8 (m16n8k16), rows i, K k' holds block m = pi(k') with
+// pi(4t + j) = 2t + j (j < 2), 8 + 2t + (j - 2) (j >= 2) -- the m order in
+// which the bytes sit in a lane's k32 B fragment (see tk_stages.cuh); the
+// data byte is x + 128 (low byte xor 0x80) and c1b holds the
+// (-128 * rowsum) mod q correction.
 struct FwdFrags {
   uint32_t s1[2][32][4];
   int32_t c1[32][2];
   uint32_t s2[16][2][32][2];
+  uint32_t s1b[2][32][2];
+  int32_t c1b[32][2];
 };
 
 // Inverse stage A: per block m and parity s, A = 16x16 s8; rows as in forward
@@ -91,5 +99,7 @@ void build_inv_frags(const Matrices& M, InvFrags* F);
 
 // Slot order inside a forward stage-2 parity half.
 inline int fwd_slot_e(int slot) { return (slot >> 1) + 4 * (slot & 1); }
+// Block m of single-limb stage-1 K position k (FwdFrags::s1b).
+int basic_k_block(int k);
 
 }  // namespace tk

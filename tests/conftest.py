@@ -43,5 +43,13 @@ def cuda():
     return torch
 
 
+@pytest.fixture(scope="session")
+def golden():
+    """The committed golden vectors (outputs of the reference's own C)."""
+    import numpy as np
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_vectors.npz")
+    return dict(np.load(path))
+
+
 def rng(seed):
     return np.random.default_rng(seed)

@@ -49,7 +49,17 @@ class FwdModel:
         w = np.asarray(words, dtype=np.uint32)
         s1 = w[:256].reshape(2, 32, 4)
         c1 = w[256:320].view(np.int32).reshape(32, 2)
-        s2 = w[320:].reshape(16, 2, 32, 2)
+        s2 = w[320:2368].reshape(16, 2, 32, 2)
+        s1b = w[2368:2496].reshape(2, 32, 2)
+        c1b = w[2496:2560].view(np.int32).reshape(32, 2)
+        # single-limb stage 1: A columns k' hold block m = pi(k')
+        self.A1b = [unpack_k16(s1b[g]) for g in range(2)]
+        self.corr_b = np.zeros(16, dtype=np.int64)
+        for lane in range(32):
+            self.corr_b[lane // 4] = c1b[lane][0]
+            self.corr_b[lane // 4 + 8] = c1b[lane][1]
+        self.pi = [(2 * (k >> 2) + (k & 3)) if (k & 3) < 2 else (8 + 2 * (k >> 2) + (k & 3) - 2)
+                   for k in range(16)]
         self.A1 = [unpack_k32(s1[g]) for g in range(2)]
         corr = np.zeros(16, dtype=np.int64)
         for lane in range(32):
@@ -58,13 +68,22 @@ class FwdModel:
         self.corr = corr
         self.A2 = [[unpack_k16(s2[b][s]) for s in range(2)] for b in range(16)]
 
-    def __call__(self, x: np.ndarray) -> np.ndarray:
+    def __call__(self, x: np.ndarray, single_limb: bool = False) -> np.ndarray:
+        """single_limb: the stage-1 form for inputs in [-128, 127] (one data
+        byte x + 128 per coefficient, K in the pi order of the fragments)."""
         x = np.asarray(x, dtype=np.int16).reshape(-1, 256)
         P = x.shape[0]
-        u = (x.view(np.uint16).astype(np.int64) ^ 0x8000).reshape(P, 16, 16)  # [p][m][c]
-        X = np.stack([u & 255, u >> 8], axis=2).reshape(P, 32, 16)         # [p][k=2m+b][c]
-        D0 = self.corr[None, :, None] + np.einsum("ik,pkc->pic", self.A1[0], X)
-        D1 = np.einsum("ik,pkc->pic", self.A1[1], X)
+        if single_limb:
+            assert x.min() >= -128 and x.max() <= 127
+            u = (x.astype(np.int64) + 128).reshape(P, 16, 16)                # [p][m][c]
+            X = u[:, self.pi, :]                                             # [p][k'][c]
+            D0 = self.corr_b[None, :, None] + np.einsum("ik,pkc->pic", self.A1b[0], X)
+            D1 = np.einsum("ik,pkc->pic", self.A1b[1], X)
+        else:
+            u = (x.view(np.uint16).astype(np.int64) ^ 0x8000).reshape(P, 16, 16)  # [p][m][c]
+            X = np.stack([u & 255, u >> 8], axis=2).reshape(P, 32, 16)     # [p][k=2m+b][c]
+            D0 = self.corr[None, :, None] + np.einsum("ik,pkc->pic", self.A1[0], X)
+            D1 = np.einsum("ik,pkc->pic", self.A1[1], X)
         S = D0 + 128 * D1
         assert S.min() >= 0 and S.max() < (1 << 25), (S.min(), S.max())
         mid = S - ((S * BAR_LAZY) >> 32) * Q                                 # [p][i][c]

@@ -7,6 +7,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -134,3 +135,21 @@ def test_matvec_host_argument_errors_without_gpu(tk):
     assert L.tk_matvec_host((B * 1)(B(2, 1, None, p, None, p)), 1) == 1
     assert L.tk_matvec_host((B * 1)(B(2, 1 << 29, p, p, None, p)), 1) == 3
     assert L.tk_matvec_host((B * 1)(B(4, 1 << 27, p, p, p, p)), 1) == 3   # > 8 GiB staging
+
+
+def test_input_form_errors_without_gpu(tk):
+    L = tk.lib()
+    buf = np.zeros(8 * 256 + 16, dtype=np.int16)
+    base = (buf.ctypes.data + 15) & ~15
+    assert L.tk_ntt_small(None, None, 0, None) == 0
+    assert L.tk_ntt_small(None, base, 3, None) == 1
+    assert L.tk_ntt_small(base + 2, base + 2, 3, None) == 2
+    assert L.tk_ntt_small(base, base + 512, 2, None) == 1          # partial overlap
+    assert L.tk_ntt_packed(base, 5, base, 1, None) == 1
+    x = np.zeros((2, 256), dtype=np.int16)
+    x[1, 9] = 2                                                  # outside [-2, 1]
+    with pytest.raises(tk.TKError):
+        tk.pack_small(x, 2)
+    x[1, 9] = -2
+    p = tk.pack_small(x, 2)
+    assert p.shape == (2, 64) and p[1, 2] == (2 << 2)

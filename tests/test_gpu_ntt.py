@@ -267,3 +267,25 @@ def test_autotune_small_range(tk, cuda, oracle, tmp_path):
         check_inv(gpu_inv(tk, cuda, x), oracle.invntt(x))
     finally:
         tk.autotune_reset()
+
+
+@pytest.mark.parametrize("variant", range(3))
+def test_every_variant_many_tiles_per_cta(tk, cuda, oracle, variant):
+    """300,000 polynomials: every CTA walks tens of tiles, so each slot of
+    every variant's ring is refilled many times.  Outputs must equal the
+    default variant's byte for byte and the oracle on a sample."""
+    n = 300000
+    x = rng(5150).integers(-32768, 32768, size=(n, 256)).astype(np.int16)
+    base_f, base_i = gpu_fwd(tk, cuda, x), gpu_inv(tk, cuda, x)
+    try:
+        tk.set_variant(tk.FORWARD, variant)
+        tk.set_variant(tk.INVERSE, variant)
+        f, i = gpu_fwd(tk, cuda, x), gpu_inv(tk, cuda, x)
+    finally:
+        tk.set_variant(tk.FORWARD, -1)
+        tk.set_variant(tk.INVERSE, -1)
+    assert (f == base_f).all() and (i == base_i).all()
+    rows = rng(1).choice(n, 1500, replace=False)
+    ref_in = canon(x[rows]).astype(np.int16)
+    check_fwd(f[rows], oracle.ntt(ref_in))
+    check_inv(i[rows], oracle.invntt(ref_in))

@@ -125,3 +125,21 @@ def test_matvec_job_composition(oracle):
                 acc += oracle.poly_basemul(A[i * k + j], shat[j])
             want = canon(oracle.invntt(canon(acc).astype(np.int16)[None])[0].astype(np.int64) + e[i])
             assert (canon(got[i]) == want).all()
+
+
+def test_pack_small_format(oracle):
+    """TC-PACK byte layout (ntt_bench/ntt_bench.cu:744-752): coefficient i in
+    byte i/(8/bits), field at bit (i % (8/bits))*bits, two's complement."""
+    x = np.zeros((1, 256), dtype=np.int16)
+    x[0, :4] = [1, -1, 0, -2]
+    p2 = oracle.pack_small(2, x)
+    assert p2.shape == (1, 64) and p2[0, 0] == (1 | 3 << 2 | 0 << 4 | 2 << 6)
+    x[0, :2] = [3, -4]
+    p3 = oracle.pack_small(3, x)
+    assert p3.shape == (1, 128) and p3[0, 0] == (3 | 4 << 3)
+
+
+@pytest.mark.parametrize("bits,lo,hi", [(2, -2, 2), (3, -4, 4)])
+def test_pack_unpack_roundtrip(oracle, bits, lo, hi):
+    x = np.random.default_rng(bits).integers(lo, hi, size=(50, 256)).astype(np.int16)
+    assert (oracle.unpack_small(bits, oracle.pack_small(bits, x)) == x).all()

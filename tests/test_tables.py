@@ -73,3 +73,13 @@ def test_kernel_model_extreme_rows(tk, oracle):
     ref_in = canon(x).astype(np.int16)
     assert (fw(x) == canon(oracle.ntt(ref_in))).all()
     assert (canon(iv(x)) == canon(oracle.invntt(ref_in))).all()
+
+
+@pytest.mark.parametrize("lo,hi", [(-128, 128), (-3, 4), (-1, 2)])
+def test_single_limb_stage1_model(tk, oracle, lo, hi):
+    """The single-limb stage-1 fragments (inputs in [-128, 127]) give the same
+    transform as the reference's ntt, extremes included."""
+    fw = KM.FwdModel(tk.get_table(4))
+    x = rng(7 + hi).integers(lo, hi, size=(200, 256)).astype(np.int16)
+    x[0], x[1] = lo, hi - 1
+    assert (fw(x, single_limb=True) == canon(oracle.ntt(x))).all()
