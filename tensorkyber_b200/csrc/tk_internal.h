@@ -24,6 +24,7 @@ struct DeviceInfo {
   int cc_major = 0, cc_minor = 0;
   int mma_ctas_per_sm[2][kNumMmaVariants] = {{1, 1, 1}, {1, 1, 1}};  // [inverse][variant]
   int form_ctas_per_sm[kNumInputForms] = {1, 1, 1};  // forward input forms 1..3
+  int add_ctas_per_sm[kNumMmaVariants] = {1, 1, 1};   // inverse with addend
   size_t total_mem = 0;
 };
 

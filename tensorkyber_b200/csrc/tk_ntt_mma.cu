@@ -133,10 +133,10 @@ __device__ __forceinline__ void block_stage(uint32_t slot, uint8_t* slotp, int b
 }
 
 // Stage over m for this warp's 8 polynomials, the next ldmatrix issued ahead.
-// Inverse only: with an addend, polynomial p of this warp (global index
-// poly0 + p) gets addend[poly0 + p] added to its output; the addend words for
+// Inverse with kAdd only: polynomial p of this warp (global index poly0 + p)
+// gets addend[poly0 + p] added to its output; the addend words for
 // polynomial p+1 are fetched while p is computed.
-template <bool kInverse>
+template <bool kInverse, bool kAdd = false>
 __device__ __forceinline__ void poly_stage(uint32_t mine, uint8_t* minep, uint32_t ldt_off,
                                            const uint32_t (&am)[2][4], int32_t cm_lo,
                                            int32_t cm_hi, uint32_t w_even, uint32_t w_odd,
@@ -144,7 +144,7 @@ __device__ __forceinline__ void poly_stage(uint32_t mine, uint8_t* minep, uint32
                                            int npoly, uint32_t add_off) {
   auto load_add = [&](int p, uint32_t (&e)[4]) {
     const int poly = poly0 + p;
-    if (kInverse && addend != nullptr && poly < npoly) {
+    if (kInverse && kAdd && poly < npoly) {
       const uint32_t* w = addend + (size_t)poly * 128 + add_off;
       e[0] = __ldg(w);
       e[1] = __ldg(w + 4);
@@ -165,7 +165,7 @@ __device__ __forceinline__ void poly_stage(uint32_t mine, uint8_t* minep, uint32
       load_add(p + 1, en);
     }
     if (kInverse)
-      stage_m<true>(am, cm_lo, cm_hi, b[0], b[1], b[2], b[3], minep + p * kRowBytes, 0, 0,
+      stage_m<true, kAdd>(am, cm_lo, cm_hi, b[0], b[1], b[2], b[3], minep + p * kRowBytes, 0, 0,
                     w_nat, e);
     else  // x ^ 0x8000 bias; the 32768 * rowsum term is cancelled by cm_lo/cm_hi
       stage_m<false>(am, cm_lo, cm_hi, b[0] ^ 0x80008000u, b[1] ^ 0x80008000u,
@@ -237,11 +237,12 @@ __device__ __forceinline__ void poly_stage_small(uint32_t mine, uint8_t* minep, 
 }
 
 // ------------------------------------------------------------ the kernel ---
-template <bool kInverse, int W, int S, int kIn = kInInt16>
+template <bool kInverse, int W, int S, int kIn = kInInt16, bool kAdd = false>
 __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
     k_ntt_mma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_out,
               int npoly, const uint32_t* __restrict__ addend) {
   static_assert(!kInverse || kIn == kInInt16, "input forms are forward only");
+  static_assert(kInverse || !kAdd, "the addend is an inverse option");
   using C = Cfg<W, S, kIn>;
   extern __shared__ __align__(128) uint8_t smem[];
   const int tid = threadIdx.x;
@@ -397,7 +398,7 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
     } else {
       block_stage<true, W>(slot, slotp, blk0, ldc_off, stc_off, ac, cc);
       cta_sync_named();
-      poly_stage<true>(mine, minep, ldt_off, am, cm_lo, cm_hi, 0, 0, w_nat, addend,
+      poly_stage<true, kAdd>(mine, minep, ldt_off, am, cm_lo, cm_hi, 0, 0, w_nat, addend,
                        8 * (u_begin + k * W + warp), npoly, 8u * g8 + q4);
       fence_proxy_async_smem();
       __syncwarp();
@@ -432,6 +433,15 @@ static const Variant kVariants[2][kNumMmaVariants] = {
     {make_variant<false, 4, 3>(), make_variant<false, 8, 3>(), make_variant<false, 4, 2>()},
     {make_variant<true, 4, 3>(), make_variant<true, 8, 3>(), make_variant<true, 4, 2>()},
 };
+// Inverse with an addend (the matrix-vector pipeline's iNTT + e), per variant;
+// the plain inverse does not carry the addend's loads and adds.
+template <int W, int S>
+constexpr Variant make_add_variant() {
+  return Variant{k_ntt_mma<true, W, S, kInInt16, true>, Cfg<W, S>::kThreads, Cfg<W, S>::kSmem,
+                 Cfg<W, S>::kTile};
+}
+static const Variant kAddVariants[kNumMmaVariants] = {
+    make_add_variant<4, 3>(), make_add_variant<8, 3>(), make_add_variant<4, 2>()};
 
 // Forward kernels for the small / packed input forms: 4 warps; 3 slots for
 // int16 rows, 2 for packed rows (their loads are 8x smaller, and the smaller
@@ -532,6 +542,17 @@ bool mma_init_device(DeviceInfo* info) {
         return false;
       info->mma_ctas_per_sm[inv][v] = per_sm > 0 ? per_sm : 1;
     }
+  for (int v = 0; v < kNumMmaVariants; v++) {
+    const Variant& V = kAddVariants[v];
+    if (cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, V.smem) !=
+        cudaSuccess)
+      return false;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, V.fn, V.threads, V.smem) !=
+        cudaSuccess)
+      return false;
+    info->add_ctas_per_sm[v] = per_sm > 0 ? per_sm : 1;
+  }
   for (int f = 0; f < kNumInputForms; f++) {
     const Variant& V = kFormVariants[f];
     if (cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, V.smem) !=
@@ -592,8 +613,11 @@ cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* d
                        long long npoly, const DeviceInfo& info, cudaStream_t stream,
                        const int16_t* addend) {
   if (variant < 0 || variant >= kNumMmaVariants) variant = 0;
-  const Variant& V = kVariants[inverse ? 1 : 0][variant];
-  const long long cap = (long long)info.num_sms * info.mma_ctas_per_sm[inverse ? 1 : 0][variant];
+  const bool add_form = inverse && addend != nullptr;
+  const Variant& V = add_form ? kAddVariants[variant] : kVariants[inverse ? 1 : 0][variant];
+  const long long cap =
+      (long long)info.num_sms *
+      (add_form ? info.add_ctas_per_sm[variant] : info.mma_ctas_per_sm[inverse ? 1 : 0][variant]);
   // TMA coordinates are 32-bit: launch at most kMaxLaunchPolys per kernel.
   for (long long done = 0; done < npoly; done += kMaxLaunchPolys) {
     const int n = (int)((npoly - done) < kMaxLaunchPolys ? (npoly - done) : kMaxLaunchPolys);

@@ -13,8 +13,10 @@ constexpr int kRowBytes = 528;  // one polynomial in shared memory: 512 B + 16 B
 
 // ------------------------------------------------ shared building blocks ----
 // Stage over m (forward stage 1 / inverse stage B) of one polynomial whose B
-// operands (ldmatrix.trans of the natural-order row) are b0..b3.
-template <bool kInverse>
+// operands (ldmatrix.trans of the natural-order row) are b0..b3.  Inverse
+// with kAdd: the addend pairs `add` are added to the output (int16
+// wrap-around); without it `add` is ignored.
+template <bool kInverse, bool kAdd = false>
 __device__ __forceinline__ void stage_m(const uint32_t (&a)[2][4], int32_t c_lo, int32_t c_hi,
                                         uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3,
                                         uint8_t* row, uint32_t w_even, uint32_t w_odd,
@@ -41,6 +43,7 @@ __device__ __forceinline__ void stage_m(const uint32_t (&a)[2][4], int32_t c_lo,
   }
   // D regs: [0] (row i, c=2q), [1] (row i, c=2q+1), [2]/[3] row i+8; n-tile 1 is c+8.
   if (kInverse) {  // natural order; plus the addend pairs (int16 wrap-around add)
+    if (kAdd) {
     y0[0] += (uint32_t)(int32_t)(int16_t)(add[0] & 0xffffu);
     y0[1] += (uint32_t)((int32_t)add[0] >> 16);
     y1[0] += (uint32_t)(int32_t)(int16_t)(add[1] & 0xffffu);
@@ -49,6 +52,7 @@ __device__ __forceinline__ void stage_m(const uint32_t (&a)[2][4], int32_t c_lo,
     y0[3] += (uint32_t)((int32_t)add[2] >> 16);
     y1[2] += (uint32_t)(int32_t)(int16_t)(add[3] & 0xffffu);
     y1[3] += (uint32_t)((int32_t)add[3] >> 16);
+    }
     *(uint32_t*)(row + w_nat) = pack2(y0[0], y0[1]);
     *(uint32_t*)(row + w_nat + 16) = pack2(y1[0], y1[1]);
     *(uint32_t*)(row + w_nat + 256) = pack2(y0[2], y0[3]);
