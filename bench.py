@@ -206,17 +206,12 @@ def run_ours(args):
 
     import tensorkyber_b200 as tk
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
+    from tensorkyber_b200 import dist as tkdist
 
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    rank, world, local = tkdist.env()
+    torch.cuda.set_device(local)
+    # one process per GPU; NCCL only carries the barrier and the timing max
+    dist = tkdist.init("nccl", 120.0, device=torch.device("cuda", local))
     tk.init(local)
     if args.variant >= 0:
         tk.set_variant(tk.FORWARD, args.variant)
@@ -268,10 +263,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     fwd_ms = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(K2)]
     inv_ms = [ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(K2)]
-    if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = tkdist.max_over_ranks(total_ms, dist, device="cuda")
     status = tk.device_status(local)
     if status:
         raise RuntimeError(f"kernel status flags {status:#x}")
@@ -289,11 +281,7 @@ def run_ours(args):
         for _ in range(args.e2e_steps):
             tk.ntt_host(h)
             tk.invntt_host(h)
-        e2e_s = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = tkdist.max_over_ranks(time.perf_counter() - t0, dist, device="cuda")
         e2e = {"value": world * n * args.e2e_steps / e2e_s, "unit": "polys/s",
                "h2d_bytes_per_step": 2 * n * 512, "d2h_bytes_per_step": 2 * n * 512,
                "steps": args.e2e_steps,

@@ -47,7 +47,15 @@ __device__ __forceinline__ uint32_t red_wide(uint32_t s) {
 
 // One warp per job; lane l owns coefficient pairs 4l .. 4l+3 (16 bytes of every
 // polynomial).  vec holds ntt(s) on entry and the accumulated products on
-// exit; all k polynomials of a job are read before any is written.
+// exit.  All k + k^2 loads of a job are issued before any arithmetic (the
+// kernel streams A from HBM and is bound by loads in flight), and the raw
+// products are accumulated first: per pair t with z = z_t,
+//   out0 = 2^-16 (sum_j a0 b0 + z sum_j a1 b1),  out1 = 2^-16 sum_j (a0 b1 + a1 b0)
+// so the constants (2^-16 and z 2^-16, g_bm_zr) are applied once per output
+// pair rather than to every ntt(s) coefficient.  |sum| < 2k * 32768 * q < 2^30
+// for k <= 4.
+constexpr uint32_t kSumBias = 3329u * 262144u;  // > 2^29.7 >= |sum|; sum + bias < 2^31
+
 template <int K>
 __global__ void __launch_bounds__(256) k_basemul_acc(const int16_t* __restrict__ A,
                                                      int16_t* __restrict__ vec, int njobs) {
@@ -60,38 +68,37 @@ __global__ void __launch_bounds__(256) k_basemul_acc(const int16_t* __restrict__
   grid_dependency_wait();
   grid_launch_dependents();
   for (int job = gw; job < njobs; job += nw) {
-    uint32_t B0[K][4], B1[K][4], Bz[K][4];
+    uint4 b[K], a[K][K];
 #pragma unroll
-    for (int j = 0; j < K; j++) {
-      const uint4 v = *(const uint4*)(vec + ((size_t)job * K + j) * 256 + 8 * lane);
-      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+    for (int j = 0; j < K; j++)
+      b[j] = *(const uint4*)(vec + ((size_t)job * K + j) * 256 + 8 * lane);
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const uint32_t b0 = w[u] & 0xffffu, b1 = w[u] >> 16;  // forward output, [0, q)
-        B0[j][u] = mulmod_lazy(b0, kRinv);
-        B1[j][u] = mulmod_lazy(b1, kRinv);
-        Bz[j][u] = mulmod_lazy(b1, zr[u]);
-      }
-    }
+    for (int i = 0; i < K; i++)
+#pragma unroll
+      for (int j = 0; j < K; j++)
+        a[i][j] = __ldcs((const uint4*)(A + (((size_t)job * K + i) * K + j) * 256 + 8 * lane));
 #pragma unroll
     for (int i = 0; i < K; i++) {
-      int32_t acc0[4] = {0, 0, 0, 0}, acc1[4] = {0, 0, 0, 0};
-#pragma unroll
-      for (int j = 0; j < K; j++) {
-        const uint4 v = __ldcs((const uint4*)(A + (((size_t)job * K + i) * K + j) * 256 + 8 * lane));
-        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const int32_t a0 = (int16_t)(w[u] & 0xffffu), a1 = (int32_t)w[u] >> 16;
-          acc0[u] += a0 * (int32_t)B0[j][u] + a1 * (int32_t)Bz[j][u];
-          acc1[u] += a0 * (int32_t)B1[j][u] + a1 * (int32_t)B0[j][u];
-        }
-      }
-      // |acc| < 2K * 32768 * (q + 8) < 2^30: bias to non-negative, reduce.
       uint32_t o[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++)
-        o[u] = pack2(red_wide((uint32_t)acc0[u] + kAccBias), red_wide((uint32_t)acc1[u] + kAccBias));
+      for (int u = 0; u < 4; u++) {
+        int32_t t00 = 0, t11 = 0, t1 = 0;
+#pragma unroll
+        for (int j = 0; j < K; j++) {
+          const uint32_t aw = u == 0 ? a[i][j].x : u == 1 ? a[i][j].y : u == 2 ? a[i][j].z : a[i][j].w;
+          const uint32_t bw = u == 0 ? b[j].x : u == 1 ? b[j].y : u == 2 ? b[j].z : b[j].w;
+          const int32_t a0 = (int16_t)(aw & 0xffffu), a1 = (int32_t)aw >> 16;
+          const int32_t b0 = (int32_t)(bw & 0xffffu), b1 = (int32_t)(bw >> 16);  // [0, q)
+          t00 += a0 * b0;
+          t11 += a1 * b1;
+          t1 += a0 * b1 + a1 * b0;
+        }
+        const uint32_t r00 = red_wide((uint32_t)t00 + kSumBias);  // [0, 3q)
+        const uint32_t r11 = red_wide((uint32_t)t11 + kSumBias);
+        const uint32_t r1 = red_wide((uint32_t)t1 + kSumBias);
+        // r00 * 169 + r11 * zr < 3q * 169 + 3q * q < 2^31
+        o[u] = pack2(red_wide(r00 * kRinv + r11 * zr[u]), red_wide(r1 * kRinv));
+      }
       *(uint4*)(vec + ((size_t)job * K + i) * 256 + 8 * lane) = make_uint4(o[0], o[1], o[2], o[3]);
     }
   }
