@@ -249,8 +249,8 @@ def run_ours(args):
         dist.barrier()
     clocks = sampler.stop()
     total_ms = e_start.elapsed_time(e_end)
-    # per-kernel split (roofline): the same workload with an event around each
-    # launch, which serialises the launches (conservative per-kernel times)
+    # per-launch split (batch latency p50/p99): the same workload with an event
+    # around each launch, which serialises the launches
     K2 = min(K, 2000)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * K2 + 1)]
     torch.cuda.synchronize()
@@ -263,6 +263,19 @@ def run_ours(args):
     torch.cuda.synchronize()
     fwd_ms = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(K2)]
     inv_ms = [ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(K2)]
+    # per-kernel average launch duration (roofline): K2 launches of one kernel
+    # back to back between two events, batches rotated as in the timed region
+    # (each launch reads data last touched three launches earlier, > L2)
+    group_ms = {}
+    for name, fn in (("ntt_fwd", tk.ntt), ("ntt_inv", tk.invntt)):
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        g0.record(stream)
+        for k in range(K2):
+            fn(batches[k % 4], stream=stream)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        group_ms[name] = g0.elapsed_time(g1) / K2
     total_ms = tkdist.max_over_ranks(total_ms, dist, device="cuda")
     status = tk.device_status(local)
     if status:
@@ -288,8 +301,9 @@ def run_ours(args):
                "how": "tk_ntt_host + tk_invntt_host on a pinned host batch, wall clock"}
 
     if rank == 0:
-        fwd_avg = sum(fwd_ms) / K2
-        inv_avg = sum(inv_ms) / K2
+        fwd_iso = sum(fwd_ms) / K2
+        inv_iso = sum(inv_ms) / K2
+        fwd_avg, inv_avg = group_ms["ntt_fwd"], group_ms["ntt_inv"]
         dom, avg = ("ntt_fwd", fwd_avg) if fwd_avg >= inv_avg else ("ntt_inv", inv_avg)
         peak, peak_kind = load_peak()
         achieved = BYTES_PER_POLY * n / (avg * 1e-3) / 1e9
@@ -309,7 +323,10 @@ def run_ours(args):
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_kind == "measured" else "fallback 6650 GB/s",
                          "bytes_per_launch": BYTES_PER_POLY * n},
-            "kernels_ms": {"ntt_fwd_avg": fwd_avg, "ntt_inv_avg": inv_avg},
+            "kernels_ms": {"ntt_fwd_avg": fwd_avg, "ntt_inv_avg": inv_avg,
+                           "ntt_fwd_isolated": fwd_iso, "ntt_inv_isolated": inv_iso,
+                           "how": "avg: K2 launches of one kernel back to back between two "
+                                  "events; isolated: an event around every launch"},
             "kernel_variant": {"forward": tk.variant_name(tk.get_variant(tk.FORWARD, n)),
                                "inverse": tk.variant_name(tk.get_variant(tk.INVERSE, n))},
             "latency_us": {"batch_roundtrip_p50": 1e3 * lat_rt[len(lat_rt) // 2],

@@ -482,16 +482,24 @@ static int launch_matvec_batches(const tk_matvec_batch* batches, int nbatches,
     }
     return TK_SUCCESS;
   }
-  for (int b = 0; b < nbatches; b++) {
-    const tk_matvec_batch& B = batches[b];
-    if (B.njobs == 0) continue;
-    const long long chunk = g_matvec_chunk.load(std::memory_order_relaxed);
-    cudaError_t e = tk::launch_matvec(B.k, B.njobs, B.A, B.s, B.e, B.out, *info,
-                                      (cudaStream_t)stream, choose_variant(false, (size_t)chunk),
-                                      choose_variant(true, (size_t)chunk), chunk);
-    if (e != cudaSuccess) {
-      set_launch_err(e);
-      return TK_ERR_CUDA;
+  // non-empty batches, up to kMaxSegs per pipeline call (they share its NTT launches)
+  const long long chunk = g_matvec_chunk.load(std::memory_order_relaxed);
+  tk::MatvecPart parts[tk::kMaxSegs];
+  int np = 0;
+  for (int b = 0; b <= nbatches; b++) {
+    if (b < nbatches && batches[b].njobs != 0) {
+      const tk_matvec_batch& B = batches[b];
+      parts[np++] = tk::MatvecPart{B.k, B.njobs, B.A, B.s, B.e, B.out};
+    }
+    if (np == tk::kMaxSegs || (b == nbatches && np > 0)) {
+      cudaError_t e = tk::launch_matvec(parts, np, *info, stream,
+                                        choose_variant(false, (size_t)chunk),
+                                        choose_variant(true, (size_t)chunk), chunk);
+      if (e != cudaSuccess) {
+        set_launch_err(e);
+        return TK_ERR_CUDA;
+      }
+      np = 0;
     }
   }
   return TK_SUCCESS;

@@ -39,6 +39,22 @@ cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* d
                        long long npoly, const DeviceInfo& info, cudaStream_t stream,
                        const int16_t* addend = nullptr);
 
+// One batch of a multi-batch launch: npoly polynomials src -> dst (src == dst
+// for in place); inverse only: an optional addend.
+struct Seg {
+  const int16_t* src;
+  int16_t* dst;
+  long long npoly;
+  const int16_t* addend;
+};
+constexpr int kMaxSegs = 4;  // batches per kernel launch
+// Transforms every segment, packing up to kMaxSegs of them (pieces of at
+// most kMaxLaunchPolys) into each kernel launch, so several small batches
+// fill the GPU like one large one.  A segment with an addend selects the
+// inverse-with-addend kernel for its launch (segments without one add nothing).
+cudaError_t launch_mma_segs(bool inverse, int variant, const Seg* segs, int nseg,
+                            const DeviceInfo& info, cudaStream_t stream);
+
 // CUresult of the calling thread's last tensor-map encode (launch_mma reports
 // cudaErrorInvalidResourceHandle when an encode failed).
 int last_encode_result();
@@ -60,8 +76,18 @@ struct FusedBatches {
 };
 cudaError_t launch_matvec_fused(const FusedBatches& args, const DeviceInfo& info,
                                 cudaStream_t stream);
-cudaError_t launch_matvec(int k, size_t njobs, const int16_t* A, const int16_t* s,
-                          const int16_t* e, int16_t* out, const DeviceInfo& info,
+// One uniform-k batch of device buffers for the three-kernel pipeline.
+struct MatvecPart {
+  int k;
+  size_t njobs;
+  const int16_t* A;
+  const int16_t* s;
+  const int16_t* e;
+  int16_t* out;
+};
+// The pipeline over up to kMaxSegs batches (forward NTT, basemul-accumulate,
+// inverse NTT + e per chunk of at most chunk_vec_polys vector polynomials).
+cudaError_t launch_matvec(const MatvecPart* batches, int nb, const DeviceInfo& info,
                           cudaStream_t stream, int fwd_variant, int inv_variant,
                           long long chunk_vec_polys);
 

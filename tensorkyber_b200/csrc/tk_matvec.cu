@@ -7,10 +7,13 @@
 // restates the composition (barrett of the k-term sum before invntt, as ML-KEM's
 // polyvec_basemul_acc_montgomery does).
 //
-// Execution, per uniform-k batch, in chunks of jobs whose vectors fit in L2:
-//   1. forward NTT  s -> out           (k_ntt_mma, out of place)
-//   2. basemul-acc  out <- A o out     (k_basemul_acc, in place per job)
-//   3. inverse NTT  out -> out + e     (k_ntt_mma with addend)
+// Execution, in chunks of jobs whose vectors fit in L2 (a chunk draws jobs
+// from all uniform-k batches of the call, one piece per batch):
+//   1. forward NTT  s -> out           (k_ntt_mma, out of place, all pieces in
+//                                       one launch)
+//   2. basemul-acc  out <- A o out     (k_basemul_acc<k>, in place per job, one
+//                                       launch per piece)
+//   3. inverse NTT  out -> out + e     (k_ntt_mma with addend, one launch)
 // Steps 2 and 3 read the previous step's output from L2 (a chunk holds a
 // bounded number of vector polynomials), so HBM sees A, s and e read once and out
 // written once, the traffic of a single fused kernel, and no scratch memory
@@ -593,25 +596,57 @@ static cudaError_t launch_basemul(const int16_t* A, int16_t* vec, int njobs, con
   return cudaLaunchKernelEx(&cfg, k_basemul_acc<K>, A, vec, njobs);
 }
 
-cudaError_t launch_matvec(int k, size_t njobs, const int16_t* A, const int16_t* s,
-                          const int16_t* e, int16_t* out, const DeviceInfo& info,
+cudaError_t launch_matvec(const MatvecPart* batches, int nb, const DeviceInfo& info,
                           cudaStream_t stream, int fwd_variant, int inv_variant,
                           long long chunk_vec_polys) {
-  size_t per_chunk = (size_t)chunk_vec_polys / (size_t)k;
-  if (per_chunk < 1) per_chunk = 1;
-  for (size_t j0 = 0; j0 < njobs; j0 += per_chunk) {
-    const size_t nj = (njobs - j0) < per_chunk ? (njobs - j0) : per_chunk;
-    const size_t v0 = j0 * (size_t)k * 256, a0 = j0 * (size_t)k * (size_t)k * 256;
-    const long long nvec = (long long)(nj * (size_t)k);
-    cudaError_t err = launch_mma(false, fwd_variant, s + v0, out + v0, nvec, info, stream);
-    if (err != cudaSuccess) return err;
-    switch (k) {
-      case 2: err = launch_basemul<2>(A + a0, out + v0, (int)nj, info, stream); break;
-      case 3: err = launch_basemul<3>(A + a0, out + v0, (int)nj, info, stream); break;
-      default: err = launch_basemul<4>(A + a0, out + v0, (int)nj, info, stream); break;
+  if (nb > kMaxSegs) return cudaErrorInvalidValue;
+  // chunks of at most chunk_vec_polys vector polynomials, drawn from the
+  // batches in order; a chunk holds at most one contiguous piece per batch
+  size_t cur[kMaxSegs] = {0, 0, 0, 0};
+  int b = 0;
+  while (b < nb) {
+    struct Piece {
+      int b;
+      size_t j0, nj;
+    } pieces[kMaxSegs];
+    int np = 0;
+    long long room = chunk_vec_polys;
+    while (b < nb && room > 0) {
+      const MatvecPart& B = batches[b];
+      if (cur[b] >= B.njobs) {
+        b++;
+        continue;
+      }
+      size_t take = (size_t)(room / B.k);
+      if (take < 1) take = 1;
+      if (take > B.njobs - cur[b]) take = B.njobs - cur[b];
+      pieces[np++] = Piece{b, cur[b], take};
+      cur[b] += take;
+      room -= (long long)take * B.k;
+      if (cur[b] >= B.njobs) b++;
     }
-    if (err != cudaSuccess) return err;
-    err = launch_mma(true, inv_variant, out + v0, out + v0, nvec, info, stream, e ? e + v0 : nullptr);
+    if (np == 0) break;
+    Seg fwd[kMaxSegs], inv[kMaxSegs];
+    for (int p = 0; p < np; p++) {
+      const MatvecPart& B = batches[pieces[p].b];
+      const size_t v0 = pieces[p].j0 * (size_t)B.k * 256;
+      const long long nvec = (long long)(pieces[p].nj * (size_t)B.k);
+      fwd[p] = Seg{B.s + v0, B.out + v0, nvec, nullptr};
+      inv[p] = Seg{B.out + v0, B.out + v0, nvec, B.e ? B.e + v0 : nullptr};
+    }
+    cudaError_t err = launch_mma_segs(false, fwd_variant, fwd, np, info, stream);
+    for (int p = 0; p < np && err == cudaSuccess; p++) {
+      const MatvecPart& B = batches[pieces[p].b];
+      const size_t v0 = pieces[p].j0 * (size_t)B.k * 256;
+      const size_t a0 = pieces[p].j0 * (size_t)B.k * (size_t)B.k * 256;
+      const int nj = (int)pieces[p].nj;
+      switch (B.k) {
+        case 2: err = launch_basemul<2>(B.A + a0, B.out + v0, nj, info, stream); break;
+        case 3: err = launch_basemul<3>(B.A + a0, B.out + v0, nj, info, stream); break;
+        default: err = launch_basemul<4>(B.A + a0, B.out + v0, nj, info, stream); break;
+      }
+    }
+    if (err == cudaSuccess) err = launch_mma_segs(true, inv_variant, inv, np, info, stream);
     if (err != cudaSuccess) return err;
   }
   return cudaSuccess;

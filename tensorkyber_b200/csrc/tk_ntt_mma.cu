@@ -59,6 +59,20 @@ __device__ FwdFrags g_fwd;
 __device__ InvFrags g_inv;
 __device__ unsigned int g_status;
 
+// The kernel parameter: up to kMaxSegs independent batches ("segments") in one
+// launch.  Units (8 polynomials) are numbered across segments: segment j owns
+// units [first_unit[j], first_unit[j+1]); its rows are addressed through its
+// own tensor maps (in, out) and, for the inverse with addend, its own addend
+// (npoly[j] polynomials).
+struct SegMaps {
+  CUtensorMap in[kMaxSegs];
+  CUtensorMap out[kMaxSegs];
+  const uint32_t* addend[kMaxSegs];
+  int npoly[kMaxSegs];
+  int first_unit[kMaxSegs + 1];
+  int nseg;
+};
+
 // Forward input forms: int16 polynomials (any value), int16 polynomials with
 // coefficients in [-128, 127] (single-limb stage 1), and packed 2- or 3-bit
 // fields (TC-PACK format, single-limb stage 1).
@@ -144,7 +158,7 @@ __device__ __forceinline__ void poly_stage(uint32_t mine, uint8_t* minep, uint32
                                            int npoly, uint32_t add_off) {
   auto load_add = [&](int p, uint32_t (&e)[4]) {
     const int poly = poly0 + p;
-    if (kInverse && kAdd && poly < npoly) {
+    if (kInverse && kAdd && addend != nullptr && poly < npoly) {
       const uint32_t* w = addend + (size_t)poly * 128 + add_off;
       e[0] = __ldg(w);
       e[1] = __ldg(w + 4);
@@ -239,8 +253,7 @@ __device__ __forceinline__ void poly_stage_small(uint32_t mine, uint8_t* minep, 
 // ------------------------------------------------------------ the kernel ---
 template <bool kInverse, int W, int S, int kIn = kInInt16, bool kAdd = false>
 __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
-    k_ntt_mma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_out,
-              int npoly, const uint32_t* __restrict__ addend) {
+    k_ntt_mma(const __grid_constant__ SegMaps segs) {
   static_assert(!kInverse || kIn == kInInt16, "input forms are forward only");
   static_assert(kInverse || !kAdd, "the addend is an inverse option");
   using C = Cfg<W, S, kIn>;
@@ -248,7 +261,7 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  const int nunits = (npoly + 7) >> 3;
+  const int nunits = segs.first_unit[segs.nseg];
   const int u_begin = (int)((long long)blockIdx.x * nunits / gridDim.x);
   const int u_end = (int)((long long)(blockIdx.x + 1) * nunits / gridDim.x);
   const int nmine = (u_end - u_begin + W - 1) / W;  // tiles of this CTA (CTA-uniform)
@@ -323,19 +336,28 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
   const uint32_t stc_off = kRowBytes * (2 * q4) + 4u * g8;  // output pair lane/4, polys 2q, 2q+1
 
   // ---- TMA issue: lane 0 of each warp moves its 8 polynomials (one box) ----
+  // segment of a unit (units are numbered across the launch's segments)
+  auto seg_of = [&](int unit) {
+    int sg = 0;
+#pragma unroll
+    for (int j = 1; j < kMaxSegs; j++) sg += (j < segs.nseg && unit >= segs.first_unit[j]);
+    return sg;
+  };
   auto issue_load = [&](int k, int slot_i) {
     if (lane != 0) return;
     const int unit = u_begin + k * W + warp;
     const uint32_t bar = bar0 + 8 * slot_i;
     if (unit < u_end) {
+      const int sg = seg_of(unit);
+      const CUtensorMap* tm_in = &segs.in[sg];
+      const int row = 8 * (unit - segs.first_unit[sg]);
       if (C::kPackBytes) {  // the packed rows, after the tile's padded rows
         mbar_expect_tx(bar, 8 * C::kPackBytes);
         tma_load_2d(smem0 + slot_i * C::kSlotBytes + C::kRowsBytes + warp * 8 * C::kPackBytes,
-                    &tm_in, 0, 8 * unit, bar);
+                    tm_in, 0, row, bar);
       } else {
         mbar_expect_tx(bar, kWarpBoxBytes);
-        tma_load_2d(smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes, &tm_in, 0, 8 * unit,
-                    bar);
+        tma_load_2d(smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes, tm_in, 0, row, bar);
       }
     } else {
       mbar_expect_tx(bar, 0);  // arrive only
@@ -344,8 +366,11 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
   auto issue_store = [&](int k, int slot_i) {
     if (lane != 0) return;
     const int unit = u_begin + k * W + warp;
-    if (unit < u_end)
-      tma_store_2d(&tm_out, 0, 8 * unit, smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes);
+    if (unit < u_end) {
+      const int sg = seg_of(unit);
+      tma_store_2d(&segs.out[sg], 0, 8 * (unit - segs.first_unit[sg]),
+                   smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes);
+    }
     bulk_commit();
   };
 
@@ -398,8 +423,12 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
     } else {
       block_stage<true, W>(slot, slotp, blk0, ldc_off, stc_off, ac, cc);
       cta_sync_named();
-      poly_stage<true, kAdd>(mine, minep, ldt_off, am, cm_lo, cm_hi, 0, 0, w_nat, addend,
-                       8 * (u_begin + k * W + warp), npoly, 8u * g8 + q4);
+      const int unit = u_begin + k * W + warp;
+      const int sg = kAdd ? seg_of(unit) : 0;
+      poly_stage<true, kAdd>(mine, minep, ldt_off, am, cm_lo, cm_hi, 0, 0, w_nat,
+                             kAdd ? segs.addend[sg] : nullptr,
+                             8 * (unit - segs.first_unit[sg]), kAdd ? segs.npoly[sg] : 0,
+                             8u * g8 + q4);
       fence_proxy_async_smem();
       __syncwarp();
       issue_store(k, slot_i);
@@ -414,7 +443,7 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
 }
 
 // ------------------------------------------------------------ host side ----
-using Fn = void (*)(const CUtensorMap, const CUtensorMap, int, const uint32_t*);
+using Fn = void (*)(const SegMaps);
 
 struct Variant {
   Fn fn;
@@ -567,10 +596,10 @@ bool mma_init_device(DeviceInfo* info) {
   return true;
 }
 
-static cudaError_t launch_variant(const Variant& V, long long cap, const CUtensorMap& m_in,
-                                  const CUtensorMap& m_out, int n, const uint32_t* add,
+static cudaError_t launch_variant(const Variant& V, long long cap, const SegMaps& m,
                                   cudaStream_t stream) {
-  long long ctas = (n + V.tile - 1) / V.tile;
+  const long long polys = 8LL * m.first_unit[m.nseg];
+  long long ctas = (polys + V.tile - 1) / V.tile;
   if (ctas > cap) ctas = cap;
   if (ctas < 1) ctas = 1;
   cudaLaunchConfig_t cfg = {};
@@ -583,7 +612,7 @@ static cudaError_t launch_variant(const Variant& V, long long cap, const CUtenso
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, V.fn, m_in, m_out, n, add);
+  return cudaLaunchKernelEx(&cfg, V.fn, m);
 }
 
 cudaError_t launch_fwd_form(int form, const void* src, int16_t* dst, long long npoly,
@@ -595,43 +624,73 @@ cudaError_t launch_fwd_form(int form, const void* src, int16_t* dst, long long n
   for (long long done = 0; done < npoly; done += kMaxLaunchPolys) {
     const int n = (int)((npoly - done) < kMaxLaunchPolys ? (npoly - done) : kMaxLaunchPolys);
     const uint8_t* in = (const uint8_t*)src + done * row_bytes;
-    CUtensorMap m_in, m_out;
-    const bool ok_in = form == kInSmall ? encode_batch_map(&m_in, (const int16_t*)in, n)
-                                        : encode_packed_map(&m_in, in, n, row_bytes);
+    SegMaps m = {};
+    const bool ok_in = form == kInSmall ? encode_batch_map(&m.in[0], (const int16_t*)in, n)
+                                        : encode_packed_map(&m.in[0], in, n, row_bytes);
     if (!ok_in) return cudaErrorInvalidResourceHandle;
     if ((const void*)in == (const void*)(dst + done * 256))
-      m_out = m_in;
-    else if (!encode_batch_map(&m_out, dst + done * 256, n))
+      m.out[0] = m.in[0];
+    else if (!encode_batch_map(&m.out[0], dst + done * 256, n))
       return cudaErrorInvalidResourceHandle;
-    const cudaError_t e = launch_variant(V, cap, m_in, m_out, n, nullptr, stream);
+    m.npoly[0] = n;
+    m.first_unit[0] = 0;
+    m.first_unit[1] = (n + 7) / 8;
+    m.nseg = 1;
+    const cudaError_t e = launch_variant(V, cap, m, stream);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
 
-cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* dst,
-                       long long npoly, const DeviceInfo& info, cudaStream_t stream,
-                       const int16_t* addend) {
+cudaError_t launch_mma_segs(bool inverse, int variant, const Seg* segs, int nseg,
+                            const DeviceInfo& info, cudaStream_t stream) {
   if (variant < 0 || variant >= kNumMmaVariants) variant = 0;
-  const bool add_form = inverse && addend != nullptr;
+  bool add_form = false;
+  for (int j = 0; j < nseg; j++) add_form |= inverse && segs[j].addend != nullptr;
   const Variant& V = add_form ? kAddVariants[variant] : kVariants[inverse ? 1 : 0][variant];
   const long long cap =
       (long long)info.num_sms *
       (add_form ? info.add_ctas_per_sm[variant] : info.mma_ctas_per_sm[inverse ? 1 : 0][variant]);
-  // TMA coordinates are 32-bit: launch at most kMaxLaunchPolys per kernel.
-  for (long long done = 0; done < npoly; done += kMaxLaunchPolys) {
-    const int n = (int)((npoly - done) < kMaxLaunchPolys ? (npoly - done) : kMaxLaunchPolys);
-    CUtensorMap m_in, m_out;
-    if (!encode_batch_map(&m_in, src + done * 256, n)) return cudaErrorInvalidResourceHandle;
-    if (src == dst)
-      m_out = m_in;
-    else if (!encode_batch_map(&m_out, dst + done * 256, n))
-      return cudaErrorInvalidResourceHandle;
-    const uint32_t* add = addend ? (const uint32_t*)(addend + done * 256) : nullptr;
-    const cudaError_t e = launch_variant(V, cap, m_in, m_out, n, add, stream);
-    if (e != cudaSuccess) return e;
+  // pieces of at most kMaxLaunchPolys (TMA coordinates are 32-bit), up to
+  // kMaxSegs of them per launch
+  SegMaps m = {};
+  int units = 0;
+  auto flush = [&]() -> cudaError_t {
+    if (m.nseg == 0) return cudaSuccess;
+    m.first_unit[m.nseg] = units;
+    const cudaError_t e = launch_variant(V, cap, m, stream);
+    m = SegMaps{};
+    units = 0;
+    return e;
+  };
+  for (int j = 0; j < nseg; j++) {
+    const Seg& g = segs[j];
+    for (long long done = 0; done < g.npoly; done += kMaxLaunchPolys) {
+      const int n = (int)((g.npoly - done) < kMaxLaunchPolys ? (g.npoly - done) : kMaxLaunchPolys);
+      const int k = m.nseg;
+      if (!encode_batch_map(&m.in[k], g.src + done * 256, n)) return cudaErrorInvalidResourceHandle;
+      if (g.src == g.dst)
+        m.out[k] = m.in[k];
+      else if (!encode_batch_map(&m.out[k], g.dst + done * 256, n))
+        return cudaErrorInvalidResourceHandle;
+      m.addend[k] = g.addend ? (const uint32_t*)(g.addend + done * 256) : nullptr;
+      m.npoly[k] = n;
+      m.first_unit[k] = units;
+      units += (n + 7) / 8;
+      if (++m.nseg == kMaxSegs) {
+        const cudaError_t e = flush();
+        if (e != cudaSuccess) return e;
+      }
+    }
   }
-  return cudaSuccess;
+  return flush();
+}
+
+cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* dst,
+                       long long npoly, const DeviceInfo& info, cudaStream_t stream,
+                       const int16_t* addend) {
+  const Seg g{src, dst, npoly, addend};
+  return launch_mma_segs(inverse, variant, &g, 1, info, stream);
 }
 
 cudaError_t read_and_clear_status(unsigned* flags) {

@@ -82,6 +82,28 @@ def test_matvec_spans_several_chunks(tk, cuda, oracle, mode):
     assert tk.device_status(0) == 0
 
 
+def test_matvec_five_batches_small_chunks(tk, cuda, oracle, mode):
+    """Five batches (more than one launch's segments) with a chunk of 1000
+    vector polynomials: chunks straddle batch boundaries, and one batch has a
+    single job and no addend.  Equal to each batch run alone."""
+    spec = [(3, 301, True), (2, 1, False), (4, 260, True), (2, 517, True), (3, 9, True)]
+    items = []
+    for i, (k, n, with_e) in enumerate(spec):
+        A, s, e = make_jobs(40 + i, k, n)
+        items.append((k, A, s, e if with_e else None))
+    tk.set_option(tk.OPT_MATVEC_CHUNK_POLYS, 1000)
+    try:
+        outs = run(tk, cuda, items)
+    finally:
+        tk.set_option(tk.OPT_MATVEC_CHUNK_POLYS, 0)
+    for (k, A, s, e), out in zip(items, outs):
+        (alone,) = run(tk, cuda, [(k, A, s, e)])
+        assert (out == alone).all()
+        pick = np.unique(np.r_[0:5, A.shape[0] - 5:A.shape[0]].clip(0, A.shape[0] - 1))
+        assert (canon(out[pick]) == canon(oracle_out(oracle, k, A[pick], s[pick],
+                                                     None if e is None else e[pick]))).all()
+
+
 def test_matvec_rejects_bad_batches(tk, cuda):
     import ctypes
     t = cuda.zeros((4, 2, 256), dtype=cuda.int16, device="cuda")
