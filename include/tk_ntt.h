@@ -191,9 +191,13 @@ int tk_server_destroy(tk_server *srv, double timeout_s);
  * chunk's intermediates are meant to stay in L2); 0 restores the default.
  * TK_OPT_MATVEC_MODE: TK_MATVEC_PIPELINE (NTT, basemul-accumulate and iNTT+e
  * as three stream-ordered kernels per chunk) or TK_MATVEC_FUSED (one kernel,
- * one warp per job: every intermediate stays in shared memory). */
+ * one warp per job: every intermediate stays in shared memory).
+ * TK_OPT_HOST_CHUNK_POLYS: polynomials per copy-in / transform / copy-out
+ * chunk of tk_ntt_host / tk_invntt_host (1 .. 32768, the default; smaller chunks
+ * are slower on a B200 host link: the path runs at the link rate). */
 #define TK_OPT_MATVEC_CHUNK_POLYS 1
 #define TK_OPT_MATVEC_MODE 2
+#define TK_OPT_HOST_CHUNK_POLYS 3
 #define TK_MATVEC_PIPELINE 0
 #define TK_MATVEC_FUSED 1
 int tk_set_option(int option, long long value);

@@ -401,6 +401,7 @@ class Server:
 
 
 OPT_MATVEC_CHUNK_POLYS = 1
+OPT_HOST_CHUNK_POLYS = 3
 OPT_MATVEC_MODE = 2
 MATVEC_PIPELINE, MATVEC_FUSED = 0, 1
 

@@ -43,6 +43,11 @@ thread_local char t_err[256] = "";
 // Kernel variant choice: forced by tk_set_variant (>= 0) or picked by size.
 std::atomic<int> g_forced[2] = {{-1}, {-1}};
 std::atomic<long long> g_matvec_chunk{tk::kMatvecChunkVecPolys};
+// Host path: polynomials per chunk (TK_OPT_HOST_CHUNK_POLYS), at most the
+// staging buffers' kHostStagePolys.
+constexpr size_t kHostStagePolys = (size_t)1 << 15;  // 16 MiB per staging buffer
+constexpr long long kHostChunkDefault = 1 << 15;
+std::atomic<long long> g_host_chunk{kHostChunkDefault};
 std::atomic<int> g_matvec_mode{TK_MATVEC_PIPELINE};
 
 const char* const kVariantNames[tk::kNumMmaVariants] = {
@@ -225,7 +230,7 @@ int run_host(bool inverse, int16_t* polys, size_t npoly) {
   std::lock_guard<std::mutex> lk(S.host_mu);
   cudaError_t e;
   if (!S.stage[0]) {
-    S.stage_polys = 1u << 15;  // 16 MiB per chunk
+    S.stage_polys = kHostStagePolys;
     for (int i = 0; i < 3; i++) {
       if ((e = cudaMalloc(&S.stage[i], S.stage_polys * 512u)) != cudaSuccess ||
           (e = cudaStreamCreateWithFlags(&S.streams[i], cudaStreamNonBlocking)) != cudaSuccess) {
@@ -240,11 +245,13 @@ int run_host(bool inverse, int16_t* polys, size_t npoly) {
       }
     }
   }
+  size_t chunk = (size_t)g_host_chunk.load(std::memory_order_relaxed);
+  if (chunk > S.stage_polys) chunk = S.stage_polys;
   size_t done = 0;
   int c = 0;
   e = cudaSuccess;
   while (done < npoly && e == cudaSuccess) {
-    const size_t n = (npoly - done < S.stage_polys) ? npoly - done : S.stage_polys;
+    const size_t n = (npoly - done < chunk) ? npoly - done : chunk;
     cudaStream_t st = S.streams[c % 3];
     int16_t* buf = S.stage[c % 3];
     e = cudaMemcpyAsync(buf, polys + done * 256, n * 512u, cudaMemcpyHostToDevice, st);
@@ -805,6 +812,10 @@ int tk_set_option(int option, long long value) {
       if (value != TK_MATVEC_PIPELINE && value != TK_MATVEC_FUSED) break;
       g_matvec_mode.store((int)value);
       return TK_SUCCESS;
+    case TK_OPT_HOST_CHUNK_POLYS:
+      if (value < 0 || value > (long long)kHostStagePolys) break;
+      g_host_chunk.store(value == 0 ? kHostChunkDefault : value);
+      return TK_SUCCESS;
     default:
       break;
   }
@@ -816,6 +827,7 @@ long long tk_get_option(int option) {
   switch (option) {
     case TK_OPT_MATVEC_CHUNK_POLYS: return g_matvec_chunk.load();
     case TK_OPT_MATVEC_MODE: return g_matvec_mode.load();
+    case TK_OPT_HOST_CHUNK_POLYS: return g_host_chunk.load();
     default: return -TK_ERR_INVALID_VALUE;
   }
 }

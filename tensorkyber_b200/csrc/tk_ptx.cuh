@@ -103,7 +103,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity,
   return true;
 }
 
-// ---- tensor TMA (tiled, no multicast) ------------------------------------------
+// ---- tensor TMA (tiled, this CTA's shared memory only) -----------------------
 // tmap is the generic address of a __grid_constant__ CUtensorMap parameter.
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const void* tmap, int c0, int c1,
                                             uint32_t bar) {
