@@ -213,11 +213,18 @@ int tk_init(int device);
 
 /* Reads and clears the kernel-side error flags of a device (bit 0: forward,
  * bit 1: inverse kernel gave up on a bounded wait; bit 2: tk_ntt_small saw a
- * coefficient outside [-128, 127]).  Synchronous. */
+ * coefficient outside [-128, 127]; bit 3: tk_selftest_bounded_wait).
+ * Synchronous. */
 #define TK_FLAG_FORWARD_TIMEOUT 1u
 #define TK_FLAG_INVERSE_TIMEOUT 2u
 #define TK_FLAG_SMALL_RANGE 4u
+#define TK_FLAG_SELFTEST_TIMEOUT 8u
 int tk_device_status(int device, unsigned *flags);
+/* Exercises the kernels' give-up path: one CTA waits on an mbarrier that
+ * nothing completes, through the same bounded wait as the batch kernels, and
+ * after `seconds` (0 < seconds <= 10) sets TK_FLAG_SELFTEST_TIMEOUT and
+ * returns; the context stays usable.  Synchronous.  No reference counterpart. */
+int tk_selftest_bounded_wait(int device, double seconds);
 
 /* ---- kernel variants ------------------------------------------------------
  * The engine ships several kernel variants (CTA shape, pipeline depth) and

@@ -106,6 +106,8 @@ def lib() -> ctypes.CDLL:
     L.tk_init.restype = ctypes.c_int
     L.tk_device_status.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_uint)]
     L.tk_device_status.restype = ctypes.c_int
+    L.tk_selftest_bounded_wait.argtypes = [ctypes.c_int, ctypes.c_double]
+    L.tk_selftest_bounded_wait.restype = ctypes.c_int
     L.tk_status_string.argtypes = [ctypes.c_int]
     L.tk_status_string.restype = ctypes.c_char_p
     L.tk_last_error.argtypes = []
@@ -242,7 +244,7 @@ def invntt_host(a: np.ndarray) -> np.ndarray:
     return a
 
 
-FLAG_FORWARD_TIMEOUT, FLAG_INVERSE_TIMEOUT, FLAG_SMALL_RANGE = 1, 2, 4
+FLAG_FORWARD_TIMEOUT, FLAG_INVERSE_TIMEOUT, FLAG_SMALL_RANGE, FLAG_SELFTEST_TIMEOUT = 1, 2, 4, 8
 
 
 def ntt_small(polys, out=None, stream=None):

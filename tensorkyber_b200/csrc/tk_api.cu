@@ -748,6 +748,27 @@ int tk_init(int device) {
   return rc;
 }
 
+int tk_selftest_bounded_wait(int device, double seconds) {
+  t_err[0] = 0;
+  if (!(seconds > 0.0) || seconds > 10.0) {
+    set_msg("tk_selftest_bounded_wait: seconds must be in (0, 10]");
+    return TK_ERR_INVALID_VALUE;
+  }
+  int rc = tk_init(device);
+  if (rc) return rc;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  cudaError_t e = tk::launch_selftest_wait((unsigned long long)(seconds * 1e9), 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    set_err("tk_selftest_bounded_wait", e);
+    return TK_ERR_CUDA;
+  }
+  return TK_SUCCESS;
+}
+
 int tk_device_status(int device, unsigned* flags) {
   t_err[0] = 0;
   if (!flags) return TK_ERR_INVALID_VALUE;

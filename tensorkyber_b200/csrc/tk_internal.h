@@ -144,6 +144,9 @@ bool host_span_one_copy(const void* p, size_t bytes);
 cudaError_t launch_fwd_form(int form, const void* src, int16_t* dst, long long npoly,
                             const DeviceInfo& info, cudaStream_t stream);
 
+// One CTA that lets a bounded mbarrier wait run out (status bit 3).
+cudaError_t launch_selftest_wait(unsigned long long limit_ns, cudaStream_t stream);
+
 // Kernel-side error flags (bounded waits that gave up), read and reset.
 cudaError_t read_and_clear_status(unsigned* flags);
 

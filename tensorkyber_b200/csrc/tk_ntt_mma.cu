@@ -693,6 +693,26 @@ cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* d
   return launch_mma_segs(inverse, variant, &g, 1, info, stream);
 }
 
+// Self-test of the give-up path: one CTA waits, through the same bounded
+// wait as the batch kernels, on an mbarrier that no thread arrives at; after
+// limit_ns it sets status bit 3 and returns (the wait ends by design).
+__global__ void k_selftest_wait(unsigned long long limit_ns) {
+  __shared__ __align__(8) unsigned long long bar;
+  const uint32_t b = smem_u32(&bar);
+  if (threadIdx.x == 0) {
+    mbar_init(b, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const bool ok = mbar_wait_bounded(b, 0, limit_ns);
+  if (!__syncthreads_and(ok) && threadIdx.x == 0) atomicOr(&g_status, 8u);
+}
+
+cudaError_t launch_selftest_wait(unsigned long long limit_ns, cudaStream_t stream) {
+  k_selftest_wait<<<1, 32, 0, stream>>>(limit_ns);
+  return cudaGetLastError();
+}
+
 cudaError_t read_and_clear_status(unsigned* flags) {
   unsigned v = 0;
   cudaError_t e = cudaMemcpyFromSymbol(&v, g_status, sizeof(v));

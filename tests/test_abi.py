@@ -153,3 +153,9 @@ def test_input_form_errors_without_gpu(tk):
     x[1, 9] = -2
     p = tk.pack_small(x, 2)
     assert p.shape == (2, 64) and p[1, 2] == (2 << 2)
+
+
+def test_selftest_argument_errors(tk):
+    L = tk.lib()
+    assert L.tk_selftest_bounded_wait(0, 0.0) == 1
+    assert L.tk_selftest_bounded_wait(0, 11.0) == 1

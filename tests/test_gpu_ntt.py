@@ -289,3 +289,17 @@ def test_every_variant_many_tiles_per_cta(tk, cuda, oracle, variant):
     ref_in = canon(x[rows]).astype(np.int16)
     check_fwd(f[rows], oracle.ntt(ref_in))
     check_inv(i[rows], oracle.invntt(ref_in))
+
+
+def test_bounded_wait_gives_up_and_context_survives(tk, cuda, oracle):
+    """A wait on an mbarrier that nothing completes ends after its limit with
+    the status flag set (the batch kernels' give-up path); the device keeps
+    working afterwards."""
+    import time
+    t0 = time.perf_counter()
+    assert tk.lib().tk_selftest_bounded_wait(0, 0.02) == 0
+    assert time.perf_counter() - t0 < 5
+    assert tk.device_status(0) == tk.FLAG_SELFTEST_TIMEOUT
+    assert tk.device_status(0) == 0                         # read and cleared
+    x = rng(3).integers(0, Q, size=(100, 256)).astype(np.int16)
+    check_fwd(gpu_fwd(tk, cuda, x), oracle.ntt(x))
