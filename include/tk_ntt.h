@@ -126,14 +126,19 @@ int tk_matvec(const tk_matvec_batch *batches, int nbatches, tk_stream_t stream);
  * staging buffer per device that grows to the largest call (at most 8 GiB);
  * calls on one device are serialised.  out may alias s. */
 int tk_matvec_host(const tk_matvec_batch *batches, int nbatches);
-/* tk_matvec_host for callers that must not allocate device memory or streams
- * (no counterpart in the reference).  Staging is a static device array of
- * TK_NOALLOC_SCRATCH_BYTES that comes with the library module; a batch list
- * needing more (A + s + e + out bytes per batch, each rounded up to 256)
- * returns TK_ERR_TOO_LARGE.  The work runs on `stream` and the call returns
- * after synchronizing it; at most 16 batches.  Per device, the first call looks
- * up the array's address (cudaGetSymbolAddress): make it before any stream
- * capture.  Calls on one device that overlap in time race on the array. */
+/* tk_matvec_host for callers that must not allocate (no counterpart in the
+ * reference): services that reserve their device memory once at start-up and
+ * may not grow it per request, and latency-bound paths that cannot take the
+ * device-wide synchronisation of cudaFree or the cost of cudaMalloc and
+ * stream creation.  Staging is a static device array of
+ * TK_NOALLOC_SCRATCH_BYTES that comes with the library module (every GPU that
+ * loads the library holds it until exit); a batch list needing more (A + s +
+ * e + out bytes per batch, each rounded up to 256) returns TK_ERR_TOO_LARGE.
+ * The work runs on `stream` and the call returns after synchronizing it; at
+ * most 16 batches.  Per device, the first call looks up the array's address
+ * (cudaGetSymbolAddress, with that device current): make it before any stream
+ * capture.  The array keeps the last call's contents, which no call relies on;
+ * calls on one device that overlap in time race on it. */
 #define TK_NOALLOC_SCRATCH_BYTES (4 << 20)
 int tk_matvec_host_noalloc(const tk_matvec_batch *batches, int nbatches, tk_stream_t stream);
 
@@ -142,7 +147,7 @@ int tk_matvec_host_noalloc(const tk_matvec_batch *batches, int nbatches, tk_stre
  * resident job ring through a persistent device loop.  tk_server_submit
  * queues a request of njobs jobs of one k whose buffers are HOST memory
  * (A: njobs*k*k, s/e/out: njobs*k polynomials; e may be NULL; A, s, e laid
- * out back to back travel in one copy).  Requests are admitted in arrival order as request slots (and, for staged requests, pool
+ * out back to back travel in one copy; out may be s, must not overlap A or e).  Requests are admitted in arrival order as request slots (and, for staged requests, pool
  * memory) free up; their jobs run alongside jobs already on the GPU, and
  * results land in out before the ticket completes.
  *   - inputs: A, s, e are copied into the server's device pool of

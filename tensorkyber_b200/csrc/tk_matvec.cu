@@ -523,13 +523,7 @@ __global__ void __launch_bounds__(32 * kServeWarps, 1)
 cudaError_t launch_serve(const ServeJob* ring, uint32_t ring_mask, ServeCtl* ctl,
                          unsigned int* req_ctr, unsigned int* req_flag, unsigned long long idle_ns,
                          const DeviceInfo& info, cudaStream_t stream) {
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(k_serve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    kServeSmem);
-  });
-  if (attr_err != cudaSuccess) return attr_err;
+  // (k_serve's shared-memory attribute is set per device by matvec_init_device)
   k_serve<<<(unsigned)info.num_sms, 32 * kServeWarps, kServeSmem, stream>>>(
       ring, ring_mask, ctl, req_ctr, req_flag, idle_ns);
   return cudaGetLastError();
@@ -548,7 +542,9 @@ static bool upload_fused_tables() {
   return cudaMemcpyToSymbol(g_mv_fwd, &FF, sizeof(FF)) == cudaSuccess &&
          cudaMemcpyToSymbol(g_mv_inv, &IF, sizeof(IF)) == cudaSuccess &&
          cudaFuncSetAttribute(k_matvec_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              kFusedSmem) == cudaSuccess;
+                              kFusedSmem) == cudaSuccess &&
+         cudaFuncSetAttribute(k_serve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kServeSmem) == cudaSuccess;
 }
 
 cudaError_t launch_matvec_fused(const FusedBatches& args, const DeviceInfo& info,

@@ -513,6 +513,14 @@ int tk_server_submit(tk_server* S, int k, size_t njobs, const int16_t* A, const 
     return TK_ERR_INVALID_VALUE;
   if (njobs > kRingCap) return TK_ERR_TOO_LARGE;
   const size_t vb = njobs * (size_t)k * 512, ab = vb * (size_t)k;
+  // tk_matvec's aliasing rule: out may be s itself, must not overlap A or e
+  auto overlaps = [](const void* x, size_t nx, const void* y, size_t ny) {
+    const uintptr_t a = (uintptr_t)x, b = (uintptr_t)y;
+    return a < b + ny && b < a + nx;
+  };
+  if (overlaps(out, vb, A, ab) || (e && overlaps(out, vb, e, vb)) ||
+      ((const void*)out != (const void*)s && overlaps(out, vb, s, vb)))
+    return TK_ERR_INVALID_VALUE;
   std::unique_ptr<Request> r(new Request);
   r->k = k;
   r->njobs = njobs;

@@ -146,6 +146,10 @@ def test_server_rejects_oversized_and_bad_requests(tk, cuda):
         assert L.tk_server_submit(srv._h, 5, 1, s.ctypes.data, s.ctypes.data, None,
                                   out.ctypes.data, ctypes.byref(t)) == 1
         assert L.tk_server_wait(srv._h, 12345, 0.01) == 1
+        A, s, e = request(2, 2, 3)
+        buf = np.zeros(A.size + s.size, dtype=np.int16)
+        assert L.tk_server_submit(srv._h, 2, 3, buf.ctypes.data, s.ctypes.data, None,
+                                  buf.ctypes.data + 512, ctypes.byref(t)) == 1   # out inside A
 
 
 def test_pinned_buffers_rewritten_between_requests(tk, cuda, oracle):

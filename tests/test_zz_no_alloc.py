@@ -1,6 +1,8 @@
-"""tk_matvec_host_noalloc: the staging-in-static-scratch variant of
-tk_matvec_host.  Collected last, so it also runs after every other test has
-used the library in the same process."""
+"""tk_matvec_host_noalloc: tk_matvec_host staged in the library's static
+device array instead of memory allocated per call, for callers that reserve
+their device memory up front or cannot pay for cudaMalloc / cudaFree on a
+latency-bound path.  Collected last, so it also runs after every other test
+has used the library in the same process."""
 import numpy as np
 import pytest
 
