@@ -25,6 +25,7 @@ struct DeviceInfo {
   int mma_ctas_per_sm[2][kNumMmaVariants] = {{1, 1, 1}, {1, 1, 1}};  // [inverse][variant]
   int form_ctas_per_sm[kNumInputForms] = {1, 1, 1};  // forward input forms 1..3
   int add_ctas_per_sm[kNumMmaVariants] = {1, 1, 1};   // inverse with addend
+  int multi_ctas_per_sm[3] = {1, 1, 1};  // multi-segment forward / inverse / inverse+addend
   size_t total_mem = 0;
 };
 
@@ -50,7 +51,8 @@ struct Seg {
 constexpr int kMaxSegs = 4;  // batches per kernel launch
 // Transforms every segment, packing up to kMaxSegs of them (pieces of at
 // most kMaxLaunchPolys) into each kernel launch, so several small batches
-// fill the GPU like one large one.  A segment with an addend selects the
+// fill the GPU like one large one.  A launch of one piece uses the given
+// variant's single-batch kernel; a launch of several uses variant 0's shape.  A segment with an addend selects the
 // inverse-with-addend kernel for its launch (segments without one add nothing).
 cudaError_t launch_mma_segs(bool inverse, int variant, const Seg* segs, int nseg,
                             const DeviceInfo& info, cudaStream_t stream);

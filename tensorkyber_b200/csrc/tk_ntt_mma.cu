@@ -44,6 +44,7 @@
 #include <stdint.h>
 
 #include <mutex>
+#include <type_traits>
 
 #include "tk_internal.h"
 #include "tk_ptx.cuh"
@@ -59,11 +60,18 @@ __device__ FwdFrags g_fwd;
 __device__ InvFrags g_inv;
 __device__ unsigned int g_status;
 
-// The kernel parameter: up to kMaxSegs independent batches ("segments") in one
-// launch.  Units (8 polynomials) are numbered across segments: segment j owns
+// Kernel parameters.  OneSeg: one batch (every launch but the multi-batch
+// ones), its tensor maps at fixed offsets.  SegMaps: up to kMaxSegs
+// independent batches ("segments") in one launch.  Units (8 polynomials) are numbered across segments: segment j owns
 // units [first_unit[j], first_unit[j+1]); its rows are addressed through its
 // own tensor maps (in, out) and, for the inverse with addend, its own addend
 // (npoly[j] polynomials).
+struct OneSeg {
+  CUtensorMap in;
+  CUtensorMap out;
+  const uint32_t* addend;
+  int npoly;
+};
 struct SegMaps {
   CUtensorMap in[kMaxSegs];
   CUtensorMap out[kMaxSegs];
@@ -251,9 +259,11 @@ __device__ __forceinline__ void poly_stage_small(uint32_t mine, uint8_t* minep, 
 }
 
 // ------------------------------------------------------------ the kernel ---
-template <bool kInverse, int W, int S, int kIn = kInInt16, bool kAdd = false>
+template <bool kInverse, int W, int S, int kIn = kInInt16, bool kAdd = false,
+          class Param = OneSeg>
 __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
-    k_ntt_mma(const __grid_constant__ SegMaps segs) {
+    k_ntt_mma(const __grid_constant__ Param segs) {
+  constexpr bool kMulti = std::is_same<Param, SegMaps>::value;
   static_assert(!kInverse || kIn == kInInt16, "input forms are forward only");
   static_assert(kInverse || !kAdd, "the addend is an inverse option");
   using C = Cfg<W, S, kIn>;
@@ -261,7 +271,11 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  const int nunits = segs.first_unit[segs.nseg];
+  int nunits;
+  if constexpr (kMulti)
+    nunits = segs.first_unit[segs.nseg];
+  else
+    nunits = (segs.npoly + 7) >> 3;
   const int u_begin = (int)((long long)blockIdx.x * nunits / gridDim.x);
   const int u_end = (int)((long long)(blockIdx.x + 1) * nunits / gridDim.x);
   const int nmine = (u_end - u_begin + W - 1) / W;  // tiles of this CTA (CTA-uniform)
@@ -336,12 +350,32 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
   const uint32_t stc_off = kRowBytes * (2 * q4) + 4u * g8;  // output pair lane/4, polys 2q, 2q+1
 
   // ---- TMA issue: lane 0 of each warp moves its 8 polynomials (one box) ----
-  // segment of a unit (units are numbered across the launch's segments)
-  auto seg_of = [&](int unit) {
-    int sg = 0;
+  // segment of a unit (units are numbered across the launch's segments), its
+  // first unit, and its tensor maps, addend and size
+  auto seg_of = [&](int unit) -> int {
+    if constexpr (kMulti) {
+      int sg = 0;
 #pragma unroll
-    for (int j = 1; j < kMaxSegs; j++) sg += (j < segs.nseg && unit >= segs.first_unit[j]);
-    return sg;
+      for (int j = 1; j < kMaxSegs; j++) sg += (j < segs.nseg && unit >= segs.first_unit[j]);
+      return sg;
+    } else {
+      return 0;
+    }
+  };
+  auto seg_first = [&](int sg) -> int {
+    if constexpr (kMulti) return segs.first_unit[sg]; else return 0;
+  };
+  auto map_in = [&](int sg) -> const CUtensorMap* {
+    if constexpr (kMulti) return &segs.in[sg]; else return &segs.in;
+  };
+  auto map_out = [&](int sg) -> const CUtensorMap* {
+    if constexpr (kMulti) return &segs.out[sg]; else return &segs.out;
+  };
+  auto seg_addend = [&](int sg) -> const uint32_t* {
+    if constexpr (kMulti) return segs.addend[sg]; else return segs.addend;
+  };
+  auto seg_npoly = [&](int sg) -> int {
+    if constexpr (kMulti) return segs.npoly[sg]; else return segs.npoly;
   };
   auto issue_load = [&](int k, int slot_i) {
     if (lane != 0) return;
@@ -349,8 +383,8 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
     const uint32_t bar = bar0 + 8 * slot_i;
     if (unit < u_end) {
       const int sg = seg_of(unit);
-      const CUtensorMap* tm_in = &segs.in[sg];
-      const int row = 8 * (unit - segs.first_unit[sg]);
+      const CUtensorMap* tm_in = map_in(sg);
+      const int row = 8 * (unit - seg_first(sg));
       if (C::kPackBytes) {  // the packed rows, after the tile's padded rows
         mbar_expect_tx(bar, 8 * C::kPackBytes);
         tma_load_2d(smem0 + slot_i * C::kSlotBytes + C::kRowsBytes + warp * 8 * C::kPackBytes,
@@ -368,7 +402,7 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
     const int unit = u_begin + k * W + warp;
     if (unit < u_end) {
       const int sg = seg_of(unit);
-      tma_store_2d(&segs.out[sg], 0, 8 * (unit - segs.first_unit[sg]),
+      tma_store_2d(map_out(sg), 0, 8 * (unit - seg_first(sg)),
                    smem0 + slot_i * C::kSlotBytes + warp * kWarpBoxBytes);
     }
     bulk_commit();
@@ -426,8 +460,8 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
       const int unit = u_begin + k * W + warp;
       const int sg = kAdd ? seg_of(unit) : 0;
       poly_stage<true, kAdd>(mine, minep, ldt_off, am, cm_lo, cm_hi, 0, 0, w_nat,
-                             kAdd ? segs.addend[sg] : nullptr,
-                             8 * (unit - segs.first_unit[sg]), kAdd ? segs.npoly[sg] : 0,
+                             kAdd ? seg_addend(sg) : nullptr,
+                             8 * (unit - seg_first(sg)), kAdd ? seg_npoly(sg) : 0,
                              8u * g8 + q4);
       fence_proxy_async_smem();
       __syncwarp();
@@ -443,18 +477,17 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
 }
 
 // ------------------------------------------------------------ host side ----
-using Fn = void (*)(const SegMaps);
-
 struct Variant {
-  Fn fn;
+  const void* fn;
   int threads;
   int smem;
   int tile;
 };
 
-template <bool I, int W, int S>
+template <bool I, int W, int S, int kIn = kInInt16, bool kAdd = false, class P = OneSeg>
 constexpr Variant make_variant() {
-  return Variant{k_ntt_mma<I, W, S>, Cfg<W, S>::kThreads, Cfg<W, S>::kSmem, Cfg<W, S>::kTile};
+  using C = Cfg<W, S, kIn>;
+  return Variant{(const void*)k_ntt_mma<I, W, S, kIn, kAdd, P>, C::kThreads, C::kSmem, C::kTile};
 }
 
 // [inverse][variant]
@@ -464,25 +497,23 @@ static const Variant kVariants[2][kNumMmaVariants] = {
 };
 // Inverse with an addend (the matrix-vector pipeline's iNTT + e), per variant;
 // the plain inverse does not carry the addend's loads and adds.
-template <int W, int S>
-constexpr Variant make_add_variant() {
-  return Variant{k_ntt_mma<true, W, S, kInInt16, true>, Cfg<W, S>::kThreads, Cfg<W, S>::kSmem,
-                 Cfg<W, S>::kTile};
-}
 static const Variant kAddVariants[kNumMmaVariants] = {
-    make_add_variant<4, 3>(), make_add_variant<8, 3>(), make_add_variant<4, 2>()};
+    make_variant<true, 4, 3, kInInt16, true>(), make_variant<true, 8, 3, kInInt16, true>(),
+    make_variant<true, 4, 2, kInInt16, true>()};
+// Launches over several segments (variant 0's shape): forward, inverse,
+// inverse with addend.  Kept apart so that single-batch launches carry none of
+// the segment lookup.
+static const Variant kMultiVariants[3] = {
+    make_variant<false, 4, 3, kInInt16, false, SegMaps>(),
+    make_variant<true, 4, 3, kInInt16, false, SegMaps>(),
+    make_variant<true, 4, 3, kInInt16, true, SegMaps>()};
 
 // Forward kernels for the small / packed input forms: 4 warps; 3 slots for
 // int16 rows, 2 for packed rows (their loads are 8x smaller, and the smaller
 // slots let 5 CTAs share an SM instead of 3).
-template <int kIn, int S>
-constexpr Variant make_form_variant() {
-  using C = Cfg<4, S, kIn>;
-  return Variant{k_ntt_mma<false, 4, S, kIn>, C::kThreads, C::kSmem, C::kTile};
-}
-static const Variant kFormVariants[kNumInputForms] = {make_form_variant<kInSmall, 3>(),
-                                                      make_form_variant<kInPack2, 2>(),
-                                                      make_form_variant<kInPack3, 2>()};
+static const Variant kFormVariants[kNumInputForms] = {make_variant<false, 4, 3, kInSmall>(),
+                                                      make_variant<false, 4, 2, kInPack2>(),
+                                                      make_variant<false, 4, 2, kInPack3>()};
 
 static thread_local int g_last_encode_result = 0;
 
@@ -582,6 +613,17 @@ bool mma_init_device(DeviceInfo* info) {
       return false;
     info->add_ctas_per_sm[v] = per_sm > 0 ? per_sm : 1;
   }
+  for (int m = 0; m < 3; m++) {
+    const Variant& V = kMultiVariants[m];
+    if (cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, V.smem) !=
+        cudaSuccess)
+      return false;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, V.fn, V.threads, V.smem) !=
+        cudaSuccess)
+      return false;
+    info->multi_ctas_per_sm[m] = per_sm > 0 ? per_sm : 1;
+  }
   for (int f = 0; f < kNumInputForms; f++) {
     const Variant& V = kFormVariants[f];
     if (cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, V.smem) !=
@@ -596,9 +638,9 @@ bool mma_init_device(DeviceInfo* info) {
   return true;
 }
 
-static cudaError_t launch_variant(const Variant& V, long long cap, const SegMaps& m,
+template <class P>
+static cudaError_t launch_variant(const Variant& V, long long cap, const P& m, long long polys,
                                   cudaStream_t stream) {
-  const long long polys = 8LL * m.first_unit[m.nseg];
   long long ctas = (polys + V.tile - 1) / V.tile;
   if (ctas > cap) ctas = cap;
   if (ctas < 1) ctas = 1;
@@ -612,7 +654,8 @@ static cudaError_t launch_variant(const Variant& V, long long cap, const SegMaps
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, V.fn, m);
+  void* args[1] = {(void*)&m};
+  return cudaLaunchKernelExC(&cfg, V.fn, args);
 }
 
 cudaError_t launch_fwd_form(int form, const void* src, int16_t* dst, long long npoly,
@@ -624,66 +667,89 @@ cudaError_t launch_fwd_form(int form, const void* src, int16_t* dst, long long n
   for (long long done = 0; done < npoly; done += kMaxLaunchPolys) {
     const int n = (int)((npoly - done) < kMaxLaunchPolys ? (npoly - done) : kMaxLaunchPolys);
     const uint8_t* in = (const uint8_t*)src + done * row_bytes;
-    SegMaps m = {};
-    const bool ok_in = form == kInSmall ? encode_batch_map(&m.in[0], (const int16_t*)in, n)
-                                        : encode_packed_map(&m.in[0], in, n, row_bytes);
+    OneSeg m = {};
+    const bool ok_in = form == kInSmall ? encode_batch_map(&m.in, (const int16_t*)in, n)
+                                        : encode_packed_map(&m.in, in, n, row_bytes);
     if (!ok_in) return cudaErrorInvalidResourceHandle;
     if ((const void*)in == (const void*)(dst + done * 256))
-      m.out[0] = m.in[0];
-    else if (!encode_batch_map(&m.out[0], dst + done * 256, n))
+      m.out = m.in;
+    else if (!encode_batch_map(&m.out, dst + done * 256, n))
       return cudaErrorInvalidResourceHandle;
-    m.npoly[0] = n;
-    m.first_unit[0] = 0;
-    m.first_unit[1] = (n + 7) / 8;
-    m.nseg = 1;
-    const cudaError_t e = launch_variant(V, cap, m, stream);
+    m.npoly = n;
+    const cudaError_t e = launch_variant(V, cap, m, n, stream);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
+
+// One piece (at most kMaxLaunchPolys polynomials: TMA coordinates are 32-bit).
+struct Piece {
+  const int16_t* src;
+  int16_t* dst;
+  int n;
+  const int16_t* addend;
+};
 
 cudaError_t launch_mma_segs(bool inverse, int variant, const Seg* segs, int nseg,
                             const DeviceInfo& info, cudaStream_t stream) {
   if (variant < 0 || variant >= kNumMmaVariants) variant = 0;
   bool add_form = false;
   for (int j = 0; j < nseg; j++) add_form |= inverse && segs[j].addend != nullptr;
-  const Variant& V = add_form ? kAddVariants[variant] : kVariants[inverse ? 1 : 0][variant];
-  const long long cap =
-      (long long)info.num_sms *
-      (add_form ? info.add_ctas_per_sm[variant] : info.mma_ctas_per_sm[inverse ? 1 : 0][variant]);
-  // pieces of at most kMaxLaunchPolys (TMA coordinates are 32-bit), up to
-  // kMaxSegs of them per launch
-  SegMaps m = {};
-  int units = 0;
-  auto flush = [&]() -> cudaError_t {
-    if (m.nseg == 0) return cudaSuccess;
-    m.first_unit[m.nseg] = units;
-    const cudaError_t e = launch_variant(V, cap, m, stream);
-    m = SegMaps{};
-    units = 0;
-    return e;
+  // pieces of at most kMaxLaunchPolys, in order
+  Piece pc[kMaxSegs];
+  int np = 0;
+  auto launch_pieces = [&]() -> cudaError_t {
+    if (np == 0) return cudaSuccess;
+    if (np == 1) {  // one batch: the compact single-segment kernels
+      const Variant& V = add_form ? kAddVariants[variant] : kVariants[inverse ? 1 : 0][variant];
+      const long long cap = (long long)info.num_sms *
+                            (add_form ? info.add_ctas_per_sm[variant]
+                                      : info.mma_ctas_per_sm[inverse ? 1 : 0][variant]);
+      OneSeg m = {};
+      if (!encode_batch_map(&m.in, pc[0].src, pc[0].n)) return cudaErrorInvalidResourceHandle;
+      if (pc[0].src == pc[0].dst)
+        m.out = m.in;
+      else if (!encode_batch_map(&m.out, pc[0].dst, pc[0].n))
+        return cudaErrorInvalidResourceHandle;
+      m.addend = (const uint32_t*)pc[0].addend;
+      m.npoly = pc[0].n;
+      np = 0;
+      return launch_variant(V, cap, m, m.npoly, stream);
+    }
+    const int which = !inverse ? 0 : add_form ? 2 : 1;
+    const Variant& V = kMultiVariants[which];
+    const long long cap = (long long)info.num_sms * info.multi_ctas_per_sm[which];
+    SegMaps m = {};
+    int units = 0;
+    for (int k = 0; k < np; k++) {
+      if (!encode_batch_map(&m.in[k], pc[k].src, pc[k].n)) return cudaErrorInvalidResourceHandle;
+      if (pc[k].src == pc[k].dst)
+        m.out[k] = m.in[k];
+      else if (!encode_batch_map(&m.out[k], pc[k].dst, pc[k].n))
+        return cudaErrorInvalidResourceHandle;
+      m.addend[k] = (const uint32_t*)pc[k].addend;
+      m.npoly[k] = pc[k].n;
+      m.first_unit[k] = units;
+      units += (pc[k].n + 7) / 8;
+    }
+    m.first_unit[np] = units;
+    m.nseg = np;
+    np = 0;
+    return launch_variant(V, cap, m, 8LL * units, stream);
   };
   for (int j = 0; j < nseg; j++) {
     const Seg& g = segs[j];
     for (long long done = 0; done < g.npoly; done += kMaxLaunchPolys) {
       const int n = (int)((g.npoly - done) < kMaxLaunchPolys ? (g.npoly - done) : kMaxLaunchPolys);
-      const int k = m.nseg;
-      if (!encode_batch_map(&m.in[k], g.src + done * 256, n)) return cudaErrorInvalidResourceHandle;
-      if (g.src == g.dst)
-        m.out[k] = m.in[k];
-      else if (!encode_batch_map(&m.out[k], g.dst + done * 256, n))
-        return cudaErrorInvalidResourceHandle;
-      m.addend[k] = g.addend ? (const uint32_t*)(g.addend + done * 256) : nullptr;
-      m.npoly[k] = n;
-      m.first_unit[k] = units;
-      units += (n + 7) / 8;
-      if (++m.nseg == kMaxSegs) {
-        const cudaError_t e = flush();
+      pc[np++] = Piece{g.src + done * 256, g.dst + done * 256, n,
+                       g.addend ? g.addend + done * 256 : nullptr};
+      if (np == kMaxSegs) {
+        const cudaError_t e = launch_pieces();
         if (e != cudaSuccess) return e;
       }
     }
   }
-  return flush();
+  return launch_pieces();
 }
 
 cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* dst,
