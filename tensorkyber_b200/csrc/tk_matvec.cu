@@ -132,12 +132,12 @@ static bool upload_pair_constants() {
 __device__ FwdFrags g_mv_fwd;
 __device__ InvFrags g_mv_inv;
 
-// smem constants, per block pair P (blocks 2P, 2P+1) and lane: 8 words of
-// fragments (block 2P even, 2P odd, 2P+1 even, 2P+1 odd; 2 words each), and
-// for the inverse 4 accumulator-init words.
+// smem constants, per block pair P (blocks 2P, 2P+1), block h of the pair and
+// lane: 4 words of fragments (parity even, odd; 2 words each), and for the
+// inverse 4 accumulator-init words per lane.
 struct FusedConsts {
-  uint32_t fwd[8][32][8];
-  uint32_t inv[8][32][8];
+  uint32_t fwd[8][2][32][4];  // [pair][block of the pair][lane]: 16 B per lane,
+  uint32_t inv[8][2][32][4];  // lanes 16 B apart (conflict-free 128-bit loads)
   int32_t inv_c[8][32][4];
 };
 constexpr int kFusedConstBytes = (int)sizeof(FusedConsts);
@@ -152,8 +152,8 @@ __device__ __forceinline__ void fused_load_consts(FusedConsts* C) {
         const int b = 2 * P + h;
 #pragma unroll
         for (int j = 0; j < 2; j++) {
-          C->fwd[P][lane][4 * h + 2 * sp + j] = g_mv_fwd.s2[b][sp][lane][j];
-          C->inv[P][lane][4 * h + 2 * sp + j] = g_mv_inv.sa[b][sp][lane][j];
+          C->fwd[P][h][lane][2 * sp + j] = g_mv_fwd.s2[b][sp][lane][j];
+          C->inv[P][h][lane][2 * sp + j] = g_mv_inv.sa[b][sp][lane][j];
         }
         C->inv_c[P][lane][2 * h + sp] = g_mv_inv.ca[b][sp][lane];
       }
@@ -224,8 +224,8 @@ __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
     const uint32_t hbw = (P >> 1) & 1;
     uint32_t r[4];
     ldsm_x4(rows + 64u * P + row_l + 16u * (((lane >> 3) & 1) ^ hbw), r[0], r[1], r[2], r[3]);
-    const uint4 f0 = *(const uint4*)&C->fwd[P][lane][0];
-    const uint4 f1 = *(const uint4*)&C->fwd[P][lane][4];
+    const uint4 f0 = *(const uint4*)&C->fwd[P][0][lane][0];
+    const uint4 f1 = *(const uint4*)&C->fwd[P][1][lane][0];
     const uint32_t a[2][2][2] = {{{f0.x, f0.y}, {f0.z, f0.w}}, {{f1.x, f1.y}, {f1.z, f1.w}}};
     const int32_t zc[2][2] = {{0, 0}, {0, 0}};
     stage_c<false>(a, zc, r, rowp + 64 * P + stc_off);
@@ -282,8 +282,8 @@ __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
     const uint32_t x2 = r[2] ^ 0x80008000u, x3 = r[3] ^ 0x80008000u;
     const uint32_t x[4] = {__byte_perm(x0, x1, 0x5410), __byte_perm(x0, x1, 0x7632),
                            __byte_perm(x2, x3, 0x5410), __byte_perm(x2, x3, 0x7632)};
-    const uint4 f0 = *(const uint4*)&C->inv[P][lane][0];
-    const uint4 f1 = *(const uint4*)&C->inv[P][lane][4];
+    const uint4 f0 = *(const uint4*)&C->inv[P][0][lane][0];
+    const uint4 f1 = *(const uint4*)&C->inv[P][1][lane][0];
     const int4 cv = *(const int4*)&C->inv_c[P][lane][0];
     const uint32_t a[2][2][2] = {{{f0.x, f0.y}, {f0.z, f0.w}}, {{f1.x, f1.y}, {f1.z, f1.w}}};
     const int32_t ca[2][2] = {{cv.x, cv.y}, {cv.z, cv.w}};
