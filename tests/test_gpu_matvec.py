@@ -146,3 +146,20 @@ def test_matvec_host_matches_device(tk, cuda, oracle, mode):
     k, A, s, e, out = items[2]
     tk.matvec_host([(k, A, s, None, s)])                 # in place, no addend
     assert (canon(s) == canon(expect[2] - e)).all()
+
+
+def test_matvec_full_mixed_workload_sample(tk, cuda, oracle, mode):
+    """The full matrix-vector workload: 65,536 jobs, k ~ U{2,3,4}, A uniform in
+    [0, q), s and e in [-3, 3], one call with three batches; 300 sampled jobs
+    of every batch against the oracle's composition."""
+    r = rng(65536)
+    ks = r.integers(2, 5, size=65536)
+    items = []
+    for k in (2, 3, 4):
+        n = int((ks == k).sum())
+        items.append((k,) + make_jobs(900 + k, k, n))
+    outs = run(tk, cuda, items)
+    for (k, A, s, e), out in zip(items, outs):
+        pick = rng(k).choice(A.shape[0], 300, replace=False)
+        assert (canon(out[pick]) == canon(oracle_out(oracle, k, A[pick], s[pick], e[pick]))).all()
+    assert tk.device_status(0) == 0

@@ -303,3 +303,33 @@ def test_bounded_wait_gives_up_and_context_survives(tk, cuda, oracle):
     assert tk.device_status(0) == 0                         # read and cleared
     x = rng(3).integers(0, Q, size=(100, 256)).astype(np.int16)
     check_fwd(gpu_fwd(tk, cuda, x), oracle.ntt(x))
+
+
+def test_sweep_maximum_size_properties(tk, cuda):
+    """2^24 polynomials (8 GiB, the top of the batch-size sweep), checked on
+    the device through size-independent properties: invntt(ntt(x)) == 2^16 x
+    mod q for every coefficient, and linearity ntt(a + b) == ntt(a) + ntt(b)
+    mod q (both are exact identities of the transform)."""
+    torch = cuda
+    n = 1 << 24
+    g = torch.Generator(device="cuda").manual_seed(424242)
+    x = torch.randint(0, Q, (n, 256), dtype=torch.int16, device="cuda", generator=g)
+    y = x.clone()
+    tk.ntt(y)
+    tk.invntt(y)
+    step = 1 << 21
+    for i in range(0, n, step):
+        want = (x[i:i + step].to(torch.int64) * 65536) % Q
+        got = y[i:i + step].to(torch.int64) % Q
+        assert torch.equal(got, want), i
+    del y
+    a, b = x[:step], x[step:2 * step]
+    s = ((a.to(torch.int32) + b.to(torch.int32)) % Q).to(torch.int16)
+    fa, fb, fs = a.clone(), b.clone(), s
+    tk.ntt(fa)
+    tk.ntt(fb)
+    tk.ntt(fs)
+    assert torch.equal(fs.to(torch.int64) % Q,
+                       (fa.to(torch.int64) + fb.to(torch.int64)) % Q)
+    torch.cuda.synchronize()
+    assert tk.device_status(0) == 0
