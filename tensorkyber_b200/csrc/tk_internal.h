@@ -66,11 +66,13 @@ int last_encode_result();
 constexpr long long kMatvecChunkVecPolys = 131072;  // default (64 MiB); tk_set_option may change it
 bool matvec_init_device();
 // Up to three uniform-k batches for the single-launch fused kernel: global job
-// g belongs to batch b when first[b] <= g < first[b+1].
+// g belongs to batch b when first[b] <= g < first[b+1]; gfirst is the same
+// prefix over work items of floor(8 / k) jobs (filled by launch_matvec_fused).
 struct FusedBatches {
   int nb;
   int k[3];
   int first[4];
+  int gfirst[4];
   const int16_t* A[3];
   const int16_t* s[3];
   const int16_t* e[3];

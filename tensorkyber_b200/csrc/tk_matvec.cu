@@ -181,10 +181,13 @@ __device__ __forceinline__ uint32_t job_ld4(const void* p) {
   return kLoad ? __ldcv((const uint32_t*)p) : __ldcs((const uint32_t*)p);
 }
 
-// One job of width k (2..4) on this warp.  rows/rowp: the warp's 8 x 528-byte
-// buffer (smem address / pointer).
+// ng consecutive jobs of width k (2..4; ng * k <= 8) on this warp: their k*ng
+// vector polynomials fill the rows of one 8-row tile, so the block-wise stages
+// (which always run on 8 rows) are shared by the group.  A / s / e / out point
+// at the group's first job; the jobs' data are consecutive.  rows/rowp: the
+// warp's 8 x 528-byte buffer (smem address / pointer).
 template <int kLoad>
-__device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
+__device__ __forceinline__ void fused_job(int k, int ng, const int16_t* __restrict__ A,
                                           const int16_t* __restrict__ s,
                                           const int16_t* __restrict__ e, int16_t* __restrict__ out,
                                           uint32_t rows, uint8_t* rowp, const FusedConsts* C,
@@ -199,18 +202,19 @@ __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
   const uint32_t stc_off = kRowBytes * (2 * q4) + 4u * g8;
   const uint32_t zero_add[4] = {0, 0, 0, 0};
 
+  const int nrows = k * ng;
   // 1. s -> rows (each lane moves 16 bytes of every polynomial)
 #pragma unroll
-  for (int j = 0; j < 4; j++)
-    if (j < k) {
+  for (int j = 0; j < 8; j++)
+    if (j < nrows) {
       const uint4 v = job_ld16<kLoad>(s + j * 256 + 8 * lane);
       *(uint4*)(rowp + j * kRowBytes + 16 * lane) = v;
     }
   __syncwarp();
   // 2. forward stage 1 (M1), x ^ 0x8000 bias, parity-split rows
 #pragma unroll
-  for (int j = 0; j < 4; j++)
-    if (j < k) {
+  for (int j = 0; j < 8; j++)
+    if (j < nrows) {
       uint32_t b[4];
       ldsm_x4_t(rows + j * kRowBytes + ldt_off, b[0], b[1], b[2], b[3]);
       stage_m<false>(R.am_f, R.c1lo, R.c1hi, b[0] ^ 0x80008000u, b[1] ^ 0x80008000u,
@@ -231,7 +235,12 @@ __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
     stage_c<false>(a, zc, r, rowp + 64 * P + stc_off);
   }
   __syncwarp();
-  // 4. basemul-accumulate over j, accumulators in registers; acc_i -> row i
+  // 4. basemul-accumulate over j, job by job, accumulators in registers;
+  // acc_i -> the job's row i (after all of the job's rows were read)
+#pragma unroll 1
+  for (int t = 0; t < ng; t++) {
+  const int16_t* At = A + (size_t)t * k * k * 256;
+  uint8_t* rt = rowp + t * k * kRowBytes;
   int32_t acc[4][4][2];
 #pragma unroll
   for (int i = 0; i < 4; i++)
@@ -240,7 +249,7 @@ __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
 #pragma unroll
   for (int j = 0; j < 4; j++)
     if (j < k) {
-      const uint4 v = *(const uint4*)(rowp + j * kRowBytes + 16 * lane);
+      const uint4 v = *(const uint4*)(rt + j * kRowBytes + 16 * lane);
       const uint32_t w[4] = {v.x, v.y, v.z, v.w};
       uint32_t B0[4], B1[4], Bz[4];
 #pragma unroll
@@ -252,7 +261,7 @@ __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
 #pragma unroll
       for (int i = 0; i < 4; i++)
         if (i < k) {
-          const uint4 av = job_ld16<kLoad>(A + (i * k + j) * 256 + 8 * lane);
+          const uint4 av = job_ld16<kLoad>(At + (i * k + j) * 256 + 8 * lane);
           const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
 #pragma unroll
           for (int u = 0; u < 4; u++) {
@@ -270,8 +279,9 @@ __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
       for (int u = 0; u < 4; u++)
         o[u] = pack2(red_wide((uint32_t)acc[i][u][0] + kAccBias),
                      red_wide((uint32_t)acc[i][u][1] + kAccBias));
-      *(uint4*)(rowp + i * kRowBytes + 16 * lane) = make_uint4(o[0], o[1], o[2], o[3]);
+      *(uint4*)(rt + i * kRowBytes + 16 * lane) = make_uint4(o[0], o[1], o[2], o[3]);
     }
+  }
   __syncwarp();
   // 5. inverse stage A (MA), natural order in and out
 #pragma unroll 2
@@ -292,8 +302,8 @@ __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
   __syncwarp();
   // 6. inverse stage B (Minv), centred, plus e
 #pragma unroll
-  for (int j = 0; j < 4; j++)
-    if (j < k) {
+  for (int j = 0; j < 8; j++)
+    if (j < nrows) {
       uint32_t add[4] = {0, 0, 0, 0};
       if (e) {
         const uint32_t* ew = (const uint32_t*)(e + j * 256) + 8 * g8 + q4;
@@ -310,8 +320,8 @@ __device__ __forceinline__ void fused_job(int k, const int16_t* __restrict__ A,
   __syncwarp();
   // 7. rows -> out
 #pragma unroll
-  for (int j = 0; j < 4; j++)
-    if (j < k) {
+  for (int j = 0; j < 8; j++)
+    if (j < nrows) {
       const uint4 v = *(const uint4*)(rowp + j * kRowBytes + 16 * lane);
       __stcs((uint4*)(out + j * 256 + 8 * lane), v);
     }
@@ -349,16 +359,21 @@ __global__ void __launch_bounds__(32 * kFusedWarps)
   __syncthreads();
   grid_dependency_wait();
   grid_launch_dependents();
-  const int total = args.first[args.nb];
+  // work items: groups of floor(8 / k) consecutive jobs of one batch
+  const int total = args.gfirst[args.nb];
   const int gw = blockIdx.x * kFusedWarps + warp, nw = gridDim.x * kFusedWarps;
-  for (int job = gw; job < total; job += nw) {
+  for (int item = gw; item < total; item += nw) {
     int b = 0;
-    while (b + 1 < args.nb && job >= args.first[b + 1]) b++;
+    while (b + 1 < args.nb && item >= args.gfirst[b + 1]) b++;
     const int k = args.k[b];
-    const size_t t = (size_t)(job - args.first[b]);
-    fused_job<0>(k, args.A[b] + t * k * k * 256, args.s[b] + t * k * 256,
-              args.e[b] ? args.e[b] + t * k * 256 : nullptr, args.out[b] + t * k * 256, rows, rowp,
-              C, R, lane);
+    const int per = 8 / k;
+    const int j0 = (item - args.gfirst[b]) * per;
+    const int njobs = args.first[b + 1] - args.first[b];
+    const int ng = njobs - j0 < per ? njobs - j0 : per;
+    const size_t t = (size_t)j0;
+    fused_job<0>(k, ng, args.A[b] + t * k * k * 256, args.s[b] + t * k * 256,
+                 args.e[b] ? args.e[b] + t * k * 256 : nullptr, args.out[b] + t * k * 256, rows,
+                 rowp, C, R, lane);
   }
 }
 
@@ -502,7 +517,7 @@ __global__ void __launch_bounds__(32 * kServeWarps, 1)
     const int16_t* sv = (const int16_t*)(((unsigned long long)p0.w << 32) | p0.z);
     const int16_t* ev = (const int16_t*)(((unsigned long long)p1.y << 32) | p1.x);
     int16_t* out = (int16_t*)(((unsigned long long)p1.w << 32) | p1.z);
-    fused_job<1>((int)meta.x, A, sv, ev, out, rows, rowp, C, R, lane);
+    fused_job<1>((int)meta.x, 1, A, sv, ev, out, rows, rowp, C, R, lane);
     if (lane == 0) {
       // outputs may be host memory: order them system-wide before counting
       __threadfence_system();
@@ -549,7 +564,13 @@ static bool upload_fused_tables() {
 
 cudaError_t launch_matvec_fused(const FusedBatches& args, const DeviceInfo& info,
                                 cudaStream_t stream) {
-  const int total = args.first[args.nb];
+  FusedBatches a = args;  // group prefix: floor(8 / k) jobs per work item
+  a.gfirst[0] = 0;
+  for (int b = 0; b < a.nb; b++) {
+    const int per = 8 / a.k[b], n = a.first[b + 1] - a.first[b];
+    a.gfirst[b + 1] = a.gfirst[b] + (n + per - 1) / per;
+  }
+  const int total = a.gfirst[a.nb];
   if (total <= 0) return cudaSuccess;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_matvec_fused, 32 * kFusedWarps,
@@ -567,7 +588,7 @@ cudaError_t launch_matvec_fused(const FusedBatches& args, const DeviceInfo& info
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_matvec_fused, args);
+  return cudaLaunchKernelEx(&cfg, k_matvec_fused, a);
 }
 
 bool matvec_init_device() { return upload_pair_constants() && upload_fused_tables(); }
