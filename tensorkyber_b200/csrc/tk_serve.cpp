@@ -58,6 +58,11 @@ constexpr auto kSpinAfterWork = std::chrono::microseconds(2000);
 // the copy streams, so completions are never stuck behind a deep queue of
 // input copies (further requests wait, in order, on the host).
 constexpr size_t kMaxActive = 64;
+// Under load, admission waits until this many slots under kMaxActive are free
+// and then admits them in one pass, published with a single stream write:
+// otherwise every freed slot would cost its own pass (copy + publish) on the
+// serial copy stream.  Below this many active requests admission is immediate.
+constexpr size_t kAdmitBatch = 32;
 // Minimum spacing of device-loop liveness checks (an event query costs ~1 us).
 constexpr auto kLivenessPeriod = std::chrono::microseconds(20);
 
@@ -333,7 +338,9 @@ void scheduler(tk_server* S) {
     // request's first one has been (the device claims in ring order and a
     // request finishes only after all of its jobs ran).
     const unsigned long long pub0 = S->published;
-    while (err == cudaSuccess) {
+    const bool may_admit =
+        S->active.size() < kAdmitBatch || S->active.size() + kAdmitBatch <= kMaxActive;
+    while (err == cudaSuccess && may_admit) {
       const unsigned long long oldest = S->active.empty() ? S->published : S->active.front()->first;
       Request* r = nullptr;
       {
