@@ -54,10 +54,12 @@ const char* const kVariantNames[tk::kNumMmaVariants] = {
     "mma.sync 4 warps x 32-poly tiles, 3-slot TMA ring",
     "mma.sync 8 warps x 64-poly tiles, 3-slot TMA ring",
     "mma.sync 4 warps x 32-poly tiles, 2-slot TMA ring",
+    "mma.sync 4 warps x 32-poly tiles, 2-slot TMA ring, int32 stage-1 tile",
 };
 
 // Autotuned choice per direction and size bucket floor(log2(npoly)); -1 =
-// not tuned (variant 0, the fastest shape measured at every large size).
+// not tuned: variant 3 for the forward and variant 0 for the inverse, the
+// fastest shapes measured at 2^18 and 2^20 polynomials.
 constexpr int kBuckets = 33;
 std::atomic<int> g_tuned[2][kBuckets];
 struct TunedInit {
@@ -77,7 +79,7 @@ int choose_variant(bool inverse, size_t npoly) {
   const int f = g_forced[inverse ? 1 : 0].load(std::memory_order_relaxed);
   if (f >= 0) return f;
   const int t = g_tuned[inverse ? 1 : 0][size_bucket(npoly)].load(std::memory_order_relaxed);
-  return t >= 0 ? t : 0;
+  return t >= 0 ? t : (inverse ? 0 : 3);
 }
 
 void set_err(const char* what, cudaError_t e) {

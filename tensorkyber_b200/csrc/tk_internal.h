@@ -10,7 +10,9 @@ namespace tk {
 //   0: 4 warps, 32-polynomial tiles, 3 slots   (4 CTAs/SM)
 //   1: 8 warps, 64-polynomial tiles, 3 slots   (2 CTAs/SM)
 //   2: 4 warps, 32-polynomial tiles, 2 slots   (6 CTAs/SM)
-constexpr int kNumMmaVariants = 3;
+//   3: 4 warps, 32-polynomial tiles, 2 slots, forward stage 1 kept as int32
+//      sums in a shared-memory tile (3 CTAs/SM)
+constexpr int kNumMmaVariants = 4;
 // Largest batch one kernel launch covers (TMA coordinates are signed 32-bit).
 constexpr long long kMaxLaunchPolys = 1ll << 30;
 
@@ -22,9 +24,9 @@ struct DeviceInfo {
   int device = -1;
   int num_sms = 0;
   int cc_major = 0, cc_minor = 0;
-  int mma_ctas_per_sm[2][kNumMmaVariants] = {{1, 1, 1}, {1, 1, 1}};  // [inverse][variant]
+  int mma_ctas_per_sm[2][kNumMmaVariants] = {{1, 1, 1, 1}, {1, 1, 1, 1}};  // [inverse][variant]
   int form_ctas_per_sm[kNumInputForms] = {1, 1, 1};  // forward input forms 1..3
-  int add_ctas_per_sm[kNumMmaVariants] = {1, 1, 1};   // inverse with addend
+  int add_ctas_per_sm[kNumMmaVariants] = {1, 1, 1, 1};  // inverse with addend
   int multi_ctas_per_sm[3] = {1, 1, 1};  // multi-segment forward / inverse / inverse+addend
   size_t total_mem = 0;
 };

@@ -314,7 +314,7 @@ __device__ __forceinline__ void fused_job(int k, int ng, const int16_t* __restri
       }
       uint32_t b[4];
       ldsm_x4_t(rows + j * kRowBytes + ldt_off, b[0], b[1], b[2], b[3]);
-      stage_m<true, true>(R.am_i, 1664, 1664, b[0], b[1], b[2], b[3], rowp + j * kRowBytes, 0, 0, w_nat,
+      stage_m<true, true>(R.am_i, 0, 0, b[0], b[1], b[2], b[3], rowp + j * kRowBytes, 0, 0, w_nat,
                     add);
     }
   __syncwarp();

@@ -34,6 +34,14 @@
 //            read out of smem (wait_group.read), so S-1 loads stay in flight
 //            while a tile is computed
 //
+// Wide kernels (kWide): the first stage's sums are not reduced mod q; they go
+// as int32 to a tile of 1040-byte rows after the slots, and the second stage
+// reads their four bytes with m16n8k32 MMAs whose constants carry the byte
+// weights 256^j mod q.  Forward: stage 1 writes the tile by polynomial, stage
+// 2 reads it by block (the same MMA count as the k16 form).  Inverse: stage A
+// writes it by block in [c][m] order, stage B reads it by polynomial (two K
+// chunks, twice the MMAs).
+//
 // Reference counterparts: the in-place batch kernels k_ntt_2tc_tc_cc /
 // k_invntt_2tc_tc_cc / k_ntt_tc_cc_cp / k_invntt_tc_cc_cp
 // (ntt_bench/ntt_bench.cu:61-131, 181-277) over ntt_core / intt_core
@@ -90,7 +98,7 @@ constexpr int packed_row_bytes() {
   return kIn == kInPack2 ? 64 : kIn == kInPack3 ? 128 : 0;
 }
 
-template <int W, int S, int kIn = kInInt16>
+template <int W, int S, int kIn = kInInt16, bool kWide = false>
 struct Cfg {
   static constexpr int kWarps = W;
   static constexpr int kThreads = 32 * W;
@@ -100,7 +108,9 @@ struct Cfg {
   static constexpr int kRowsBytes = kTile * kRowBytes;
   static constexpr int kSlotBytes = kTile * (kRowBytes + kPackBytes);
   static constexpr int kSlots = S;
-  static constexpr int kSmem = S * kSlotBytes + 16 * S;  // slots + mbarriers
+  // wide kernels: one tile of int32 stage-1 sums after the slots
+  static constexpr int kInterBytes = kWide ? kTile * kWideRowBytes : 0;
+  static constexpr int kSmem = S * kSlotBytes + kInterBytes + 16 * S;  // + mbarriers
   static constexpr int kBlocksPerWarp = 16 / W;       // block-wise stages
   static constexpr int kPairsPerWarp = kBlocksPerWarp / 2;
   // CTAs per SM the shared memory allows; also the register cap for ptxas
@@ -151,6 +161,110 @@ __device__ __forceinline__ void block_stage(uint32_t slot, uint8_t* slotp, int b
                       slotp + nt * 8 * kRowBytes + 32 * (blk0 + 2 * p) + stc_off);
 #pragma unroll
     for (int j = 0; j < 4; j++) r[j] = n[j];
+  }
+}
+
+// Forward stage 2 from the tile's int32 intermediates (wide kernels): as
+// block_stage, two ldmatrix.x4 per block pair (one per block).  ldw[p]: this
+// lane's ldmatrix row offset of pair p's first block (polynomial lane&7 of
+// the n-tile, parity (lane/16) placed by the row swizzle, half (lane/8)&1).
+template <int W, int P>
+__device__ __forceinline__ void block_stage_wide(uint32_t inter, uint8_t* slotp, int blk0,
+                                                 const uint32_t (&ldw)[P], uint32_t stc_off,
+                                                 const uint32_t (&ac)[P][2][2][4]) {
+  constexpr int kIters = P * W;
+  uint32_t r[8];
+  ldsm_x4(inter + ldw[0], r[0], r[1], r[2], r[3]);
+  ldsm_x4(inter + ldw[0] + 64, r[4], r[5], r[6], r[7]);
+#pragma unroll
+  for (int it = 0; it < kIters; it++) {
+    const int p = it / W, nt = it % W;
+    uint32_t n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (it + 1 < kIters) {
+      const int p1 = (it + 1) / W, nt1 = (it + 1) % W;
+      const uint32_t a1 = inter + nt1 * 8 * kWideRowBytes + ldw[p1];
+      ldsm_x4(a1, n[0], n[1], n[2], n[3]);
+      ldsm_x4(a1 + 64, n[4], n[5], n[6], n[7]);
+    }
+    stage_c_wide(ac[p], r, slotp + nt * 8 * kRowBytes + 32 * (blk0 + 2 * p) + stc_off);
+#pragma unroll
+    for (int j = 0; j < 8; j++) r[j] = n[j];
+  }
+}
+
+// Inverse stage A of one tile into the int32 intermediates (wide kernels): as
+// block_stage<true>, the sums of pair p stored at offsets ia[p][s] of the rows
+// of polynomials 2q, 2q+1 of each n-tile.
+template <int W, int P>
+__device__ __forceinline__ void block_stage_inv_wide(uint32_t slot, int blk0, uint32_t ldc_off,
+                                                     uint8_t* interp, uint32_t row_off,
+                                                     const uint32_t (&ia)[P][2],
+                                                     const uint32_t (&ac)[P][2][2][2],
+                                                     const int32_t (&cc)[P][2][2]) {
+  constexpr int kIters = P * W;
+  uint32_t r[4];
+  ldsm_x4(slot + 32u * blk0 + ldc_off, r[0], r[1], r[2], r[3]);
+#pragma unroll
+  for (int it = 0; it < kIters; it++) {
+    const int p = it / W, nt = it % W;
+    uint32_t n[4] = {0, 0, 0, 0};
+    if (it + 1 < kIters) {
+      const int p1 = (it + 1) / W, nt1 = (it + 1) % W;
+      ldsm_x4(slot + nt1 * 8 * kRowBytes + 32u * (blk0 + 2 * p1) + ldc_off, n[0], n[1], n[2],
+              n[3]);
+    }
+    const uint32_t x0 = r[0] ^ 0x80008000u, x1 = r[1] ^ 0x80008000u;
+    const uint32_t x2 = r[2] ^ 0x80008000u, x3 = r[3] ^ 0x80008000u;
+    const uint32_t x[4] = {__byte_perm(x0, x1, 0x5410), __byte_perm(x0, x1, 0x7632),
+                           __byte_perm(x2, x3, 0x5410), __byte_perm(x2, x3, 0x7632)};
+    stage_c_inv_wide(ac[p], cc[p], x, interp + nt * 8 * kWideRowBytes + row_off, ia[p]);
+#pragma unroll
+    for (int j = 0; j < 4; j++) r[j] = n[j];
+  }
+}
+
+// Inverse stage B of this warp's 8 polynomials from the int32 intermediates
+// (wide kernels; irow0: the first one's row), two ldmatrix.x4 per polynomial,
+// the next one's issued ahead; addend as poly_stage.
+template <bool kAdd>
+__device__ __forceinline__ void poly_stage_inv_wide(uint32_t irow0, uint8_t* minep,
+                                                    const uint32_t (&lb)[2],
+                                                    const uint32_t (&a)[2][2][4], int32_t cm_lo,
+                                                    int32_t cm_hi, uint32_t w_nat,
+                                                    const uint32_t* addend, int poly0, int npoly,
+                                                    uint32_t add_off) {
+  auto load_add = [&](int p, uint32_t (&e)[4]) {
+    const int poly = poly0 + p;
+    if (kAdd && addend != nullptr && poly < npoly) {
+      const uint32_t* w = addend + (size_t)poly * 128 + add_off;
+      e[0] = __ldg(w);
+      e[1] = __ldg(w + 4);
+      e[2] = __ldg(w + 64);
+      e[3] = __ldg(w + 68);
+    } else {
+      e[0] = e[1] = e[2] = e[3] = 0;
+    }
+  };
+  uint32_t b[2][4], e[4];
+  ldsm_x4(irow0 + lb[0], b[0][0], b[0][1], b[0][2], b[0][3]);
+  ldsm_x4(irow0 + lb[1], b[1][0], b[1][1], b[1][2], b[1][3]);
+  load_add(0, e);
+#pragma unroll
+  for (int p = 0; p < 8; p++) {
+    uint32_t n[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}}, en[4] = {0, 0, 0, 0};
+    if (p < 7) {
+      const uint32_t nx = irow0 + (p + 1) * kWideRowBytes;
+      ldsm_x4(nx + lb[0], n[0][0], n[0][1], n[0][2], n[0][3]);
+      ldsm_x4(nx + lb[1], n[1][0], n[1][1], n[1][2], n[1][3]);
+      load_add(p + 1, en);
+    }
+    stage_m_inv_wide<kAdd>(a, cm_lo, cm_hi, b, minep + p * kRowBytes, w_nat, e);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      b[0][j] = n[0][j];
+      b[1][j] = n[1][j];
+      e[j] = en[j];
+    }
   }
 }
 
@@ -260,13 +374,14 @@ __device__ __forceinline__ void poly_stage_small(uint32_t mine, uint8_t* minep, 
 
 // ------------------------------------------------------------ the kernel ---
 template <bool kInverse, int W, int S, int kIn = kInInt16, bool kAdd = false,
-          class Param = OneSeg>
-__global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
+          class Param = OneSeg, bool kWide = false>
+__global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn, kWide>::kMinBlocks)
     k_ntt_mma(const __grid_constant__ Param segs) {
   constexpr bool kMulti = std::is_same<Param, SegMaps>::value;
   static_assert(!kInverse || kIn == kInInt16, "input forms are forward only");
   static_assert(kInverse || !kAdd, "the addend is an inverse option");
-  using C = Cfg<W, S, kIn>;
+  static_assert(!kWide || (kIn == kInInt16 && !kMulti), "wide: int16 input, one segment");
+  using C = Cfg<W, S, kIn, kWide>;
   extern __shared__ __align__(128) uint8_t smem[];
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -281,20 +396,32 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
   const int nmine = (u_end - u_begin + W - 1) / W;  // tiles of this CTA (CTA-uniform)
 
   const uint32_t smem0 = smem_u32(smem);
-  const uint32_t bar0 = smem0 + C::kSlots * C::kSlotBytes;
+  const uint32_t inter = smem0 + C::kSlots * C::kSlotBytes;  // wide: int32 intermediates
+  uint8_t* const interp = smem + C::kSlots * C::kSlotBytes;
+  const uint32_t bar0 = inter + C::kInterBytes;
 
   // ---- constants of this warp's role -> registers -------------------------
   uint32_t am[2][4];                       // stage over m (fwd M1 / inv Minv)
   int32_t cm_lo, cm_hi;                    // its accumulator init
-  uint32_t ac[C::kPairsPerWarp][2][2][2];  // block-wise stage, per (pair, block, parity)
+  constexpr int kAW = kWide && !kInverse ? 4 : 2;  // A registers (k16, or k32 wide forward)
+  uint32_t ac[C::kPairsPerWarp][2][2][kAW];  // block-wise stage, per (pair, block, parity)
   int32_t cc[C::kPairsPerWarp][2][2];      // its group-0 accumulator init
   const int blk0 = C::kBlocksPerWarp * warp;
 #pragma unroll
   for (int g = 0; g < 2; g++)
 #pragma unroll
     for (int j = 0; j < 4; j++) am[g][j] = kInverse ? g_inv.sb[g][lane][j] : g_fwd.s1[g][lane][j];
-  cm_lo = kInverse ? 1664 : g_fwd.c1[lane][0];
-  cm_hi = kInverse ? 1664 : g_fwd.c1[lane][1];
+  uint32_t amw[2][2][4];  // wide inverse stage B: [limb][K chunk]
+  if constexpr (kWide && kInverse) {
+#pragma unroll
+    for (int g = 0; g < 2; g++)
+#pragma unroll
+      for (int c = 0; c < 2; c++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) amw[g][c][j] = g_inv.sbw[g][c][lane][j];
+  }
+  cm_lo = kInverse ? 0 : g_fwd.c1[lane][0];
+  cm_hi = kInverse ? 0 : g_fwd.c1[lane][1];
   uint32_t ab[2][2] = {{0, 0}, {0, 0}};  // single-limb stage 1 (input forms)
   int32_t cb_lo = 0, cb_hi = 0;
   if (kIn != kInInt16) {
@@ -314,8 +441,10 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
       for (int s = 0; s < 2; s++) {
         const int b = blk0 + 2 * p + h;
 #pragma unroll
-        for (int j = 0; j < 2; j++)
-          ac[p][h][s][j] = kInverse ? g_inv.sa[b][s][lane][j] : g_fwd.s2[b][s][lane][j];
+        for (int j = 0; j < kAW; j++)
+          ac[p][h][s][j] = (kWide && !kInverse) ? g_fwd.s2w[b][s][lane][j]
+                           : kInverse ? g_inv.sa[b][s][lane][j & 1]
+                                      : g_fwd.s2[b][s][lane][j & 1];
         cc[p][h][s] = kInverse ? g_inv.ca[b][s][lane] : 0;
       }
 
@@ -348,6 +477,36 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
   const uint32_t ldc_off = kRowBytes * (lane & 7) + 32u * (lane >> 4) +
                            16u * (kInverse ? ((lane >> 3) & 1) : (((lane >> 3) & 1) ^ hbw));
   const uint32_t stc_off = kRowBytes * (2 * q4) + 4u * g8;  // output pair lane/4, polys 2q, 2q+1
+  // wide kernels: stage-1 stores of block lane/4 (even / odd half, swizzled),
+  // and the stage-2 ldmatrix rows of each block pair
+  const uint32_t swz1 = (uint32_t)(g8 >> 1) & 1u;
+  const uint32_t wi_e = 64u * g8 + 32u * swz1 + 8u * q4;
+  const uint32_t wi_o = 64u * g8 + 32u * (swz1 ^ 1u) + 8u * q4;
+  uint32_t ldw[C::kPairsPerWarp];
+#pragma unroll
+  for (int p = 0; p < C::kPairsPerWarp; p++) {
+    const int I = blk0 + 2 * p;
+    const uint32_t par = ((uint32_t)(lane >> 4) & 1u) ^ ((uint32_t)(I >> 1) & 1u);
+    ldw[p] = kWideRowBytes * (lane & 7) + 64u * I + 32u * par + 16u * ((lane >> 3) & 1);
+  }
+  // wide inverse: stage-A stores (rows of polynomials 2q, 2q+1; c' = 2(lane/4)
+  // + s; blocks I, I+1 side by side) and stage-B ldmatrix rows (n-tile t: row
+  // c = 8t + lane%8, 16-byte chunk lane/8 under the row swizzle)
+  const uint32_t ia_row = kWideRowBytes * (2u * q4);
+  uint32_t ia[C::kPairsPerWarp][2];
+#pragma unroll
+  for (int p = 0; p < C::kPairsPerWarp; p++) {
+    const uint32_t I = (uint32_t)(blk0 + 2 * p);
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      ia[p][s] = 64u * (2 * g8 + s) + 16u * ((I >> 2) ^ ((uint32_t)g8 & 3u)) + 4u * (I & 3u);
+  }
+  uint32_t lb[2];
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const uint32_t r = (uint32_t)lane & 7u;
+    lb[t] = 64u * (8 * t + r) + 16u * (((uint32_t)lane >> 3) ^ (r >> 1));
+  }
 
   // ---- TMA issue: lane 0 of each warp moves its 8 polynomials (one box) ----
   // segment of a unit (units are numbered across the launch's segments), its
@@ -436,7 +595,36 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn>::kMinBlocks)
     const uint32_t mine = slot + 8 * warp * kRowBytes;
     uint8_t* minep = slotp + 8 * warp * kRowBytes;
 
-    if (!kInverse) {
+    if constexpr (kWide && kInverse) {
+      block_stage_inv_wide<W>(slot, blk0, ldc_off, interp, ia_row, ia, ac, cc);
+      cta_sync_named();
+      const int unit = u_begin + k * W + warp;
+      poly_stage_inv_wide<kAdd>(inter + 8 * warp * kWideRowBytes, minep, lb, amw, cm_lo, cm_hi,
+                                w_nat, kAdd ? seg_addend(0) : nullptr, 8 * unit,
+                                kAdd ? seg_npoly(0) : 0, 8u * g8 + q4);
+      fence_proxy_async_smem();
+      __syncwarp();
+      issue_store(k, slot_i);
+    } else if constexpr (kWide) {
+      uint8_t* irow0 = interp + 8 * warp * kWideRowBytes;
+      uint32_t b[4];
+      ldsm_x4_t(mine + ldt_off, b[0], b[1], b[2], b[3]);
+#pragma unroll
+      for (int p = 0; p < 8; p++) {
+        uint32_t n[4] = {0, 0, 0, 0};
+        if (p < 7) ldsm_x4_t(mine + (p + 1) * kRowBytes + ldt_off, n[0], n[1], n[2], n[3]);
+        stage_m_wide(am, cm_lo, cm_hi, b[0] ^ 0x80008000u, b[1] ^ 0x80008000u,
+                     b[2] ^ 0x80008000u, b[3] ^ 0x80008000u, irow0 + p * kWideRowBytes, wi_e,
+                     wi_o);
+#pragma unroll
+        for (int j = 0; j < 4; j++) b[j] = n[j];
+      }
+      cta_sync_named();
+      block_stage_wide<W>(inter, slotp, blk0, ldw, stc_off, ac);
+      fence_proxy_async_smem();
+      cta_sync_named();
+      issue_store(k, slot_i);
+    } else if (!kInverse) {
       if (kIn == kInInt16)
         poly_stage<false>(mine, minep, ldt_off, am, cm_lo, cm_hi, w_even, w_odd, 0, nullptr, 0, 0,
                           0);
@@ -484,22 +672,27 @@ struct Variant {
   int tile;
 };
 
-template <bool I, int W, int S, int kIn = kInInt16, bool kAdd = false, class P = OneSeg>
+template <bool I, int W, int S, int kIn = kInInt16, bool kAdd = false, class P = OneSeg,
+          bool kWide = false>
 constexpr Variant make_variant() {
-  using C = Cfg<W, S, kIn>;
-  return Variant{(const void*)k_ntt_mma<I, W, S, kIn, kAdd, P>, C::kThreads, C::kSmem, C::kTile};
+  using C = Cfg<W, S, kIn, kWide>;
+  return Variant{(const void*)k_ntt_mma<I, W, S, kIn, kAdd, P, kWide>, C::kThreads, C::kSmem,
+                 C::kTile};
 }
 
 // [inverse][variant]
 static const Variant kVariants[2][kNumMmaVariants] = {
-    {make_variant<false, 4, 3>(), make_variant<false, 8, 3>(), make_variant<false, 4, 2>()},
-    {make_variant<true, 4, 3>(), make_variant<true, 8, 3>(), make_variant<true, 4, 2>()},
+    {make_variant<false, 4, 3>(), make_variant<false, 8, 3>(), make_variant<false, 4, 2>(),
+     make_variant<false, 4, 2, kInInt16, false, OneSeg, true>()},
+    {make_variant<true, 4, 3>(), make_variant<true, 8, 3>(), make_variant<true, 4, 2>(),
+     make_variant<true, 4, 2, kInInt16, false, OneSeg, true>()},
 };
 // Inverse with an addend (the matrix-vector pipeline's iNTT + e), per variant;
 // the plain inverse does not carry the addend's loads and adds.
 static const Variant kAddVariants[kNumMmaVariants] = {
     make_variant<true, 4, 3, kInInt16, true>(), make_variant<true, 8, 3, kInInt16, true>(),
-    make_variant<true, 4, 2, kInInt16, true>()};
+    make_variant<true, 4, 2, kInInt16, true>(),
+    make_variant<true, 4, 2, kInInt16, true, OneSeg, true>()};
 // Launches over several segments (variant 0's shape): forward, inverse,
 // inverse with addend.  Kept apart so that single-batch launches carry none of
 // the segment lookup.

@@ -158,6 +158,14 @@ __device__ __forceinline__ uint32_t red_lazy(uint32_t s) {
 __device__ __forceinline__ uint32_t red_exact(uint32_t s) {
   return s - (__umulhi(s, 82570715u) >> 6) * 3329u;
 }
+// S + (q-1)/2 < 2^26: the centred representative of S mod q, in
+// [-(q-1)/2, (q-1)/2] (two's complement): floor((S + 1664) / q) by
+// red_exact's multiplier, the offset folded into the 64-bit product's addend
+// (one multiply-add), so no separate add or subtract of 1664.
+__device__ __forceinline__ uint32_t red_centred(uint32_t s) {
+  const uint64_t x = (uint64_t)s * 82570715ull + 1664ull * 82570715ull;
+  return s - (uint32_t)(x >> 38) * 3329u;
+}
 __device__ __forceinline__ uint32_t pack2(uint32_t lo, uint32_t hi) {
   return __byte_perm(lo, hi, 0x5410);
 }

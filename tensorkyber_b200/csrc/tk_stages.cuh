@@ -10,8 +10,16 @@
 namespace tk {
 
 constexpr int kRowBytes = 528;  // one polynomial in shared memory: 512 B + 16 B pad
+// one polynomial of int32 stage-1 sums (the "wide" kernels): 1024 B + 16 B pad
+constexpr int kWideRowBytes = 1040;
 
 // ------------------------------------------------ shared building blocks ----
+template <bool kInverse, bool kAdd>
+__device__ __forceinline__ void stage_m_out(const int32_t (&lo0)[4], const int32_t (&hi0)[4],
+                                            const int32_t (&lo1)[4], const int32_t (&hi1)[4],
+                                            uint8_t* row, uint32_t w_even, uint32_t w_odd,
+                                            uint32_t w_nat, const uint32_t (&add)[4]);
+
 // Stage over m (forward stage 1 / inverse stage B) of one polynomial whose B
 // operands (ldmatrix.trans of the natural-order row) are b0..b3.  Inverse
 // with kAdd: the addend pairs `add` are added to the output (int16
@@ -28,14 +36,25 @@ __device__ __forceinline__ void stage_m(const uint32_t (&a)[2][4], int32_t c_lo,
   mma_k32(hi0, a[1], b0, b1, zero);
   mma_k32(lo1, a[0], b2, b3, cinit);
   mma_k32(hi1, a[1], b2, b3, zero);
+  stage_m_out<kInverse, kAdd>(lo0, hi0, lo1, hi1, row, w_even, w_odd, w_nat, add);
+}
+
+// Epilogue of the stage over m from its accumulators (lo / hi limb, n-tiles 0
+// and 1): forward lazy reduction to parity-split rows; inverse exact reduction,
+// centring and (kAdd) the addend, natural order.
+template <bool kInverse, bool kAdd>
+__device__ __forceinline__ void stage_m_out(const int32_t (&lo0)[4], const int32_t (&hi0)[4],
+                                            const int32_t (&lo1)[4], const int32_t (&hi1)[4],
+                                            uint8_t* row, uint32_t w_even, uint32_t w_odd,
+                                            uint32_t w_nat, const uint32_t (&add)[4]) {
   uint32_t y0[4], y1[4];
 #pragma unroll
   for (int e = 0; e < 4; e++) {
     const uint32_t s0 = (uint32_t)lo0[e] + ((uint32_t)hi0[e] << 7);
     const uint32_t s1 = (uint32_t)lo1[e] + ((uint32_t)hi1[e] << 7);
-    if (kInverse) {  // centred: accumulators carry +(q-1)/2
-      y0[e] = red_exact(s0) - 1664u;
-      y1[e] = red_exact(s1) - 1664u;
+    if (kInverse) {  // centred
+      y0[e] = red_centred(s0);
+      y1[e] = red_centred(s1);
     } else {
       y0[e] = red_lazy(s0);
       y1[e] = red_lazy(s1);
@@ -63,6 +82,60 @@ __device__ __forceinline__ void stage_m(const uint32_t (&a)[2][4], int32_t c_lo,
     *(uint32_t*)(row + w_even + 256) = pack2(y0[2], y1[2]);
     *(uint32_t*)(row + w_odd + 256) = pack2(y0[3], y1[3]);
   }
+}
+
+// Forward stage 1 without the reduction (the "wide" kernels): S = D_lo +
+// 128 D_hi, non-negative and below 2^25, goes to the polynomial's int32
+// intermediate row `irow` as it is; forward stage 2 then reads its four bytes
+// (stage_c_wide).  Row layout: block i at 64 i, its parity-s half (8 values,
+// slot order of FwdFrags::s2) at 32 (s ^ ((i >> 1) & 1)) -- the xor spreads
+// one store instruction's 8-byte lanes over all banks.  w_e / w_o: this
+// lane's offsets of block lane/4, even / odd half, slots 2q and 2q+1.
+__device__ __forceinline__ void stage_m_wide(const uint32_t (&a)[2][4], int32_t c_lo,
+                                             int32_t c_hi, uint32_t b0, uint32_t b1, uint32_t b2,
+                                             uint32_t b3, uint8_t* irow, uint32_t w_e,
+                                             uint32_t w_o) {
+  const int32_t cinit[4] = {c_lo, c_lo, c_hi, c_hi};
+  const int32_t zero[4] = {0, 0, 0, 0};
+  int32_t lo0[4], hi0[4], lo1[4], hi1[4];
+  mma_k32(lo0, a[0], b0, b1, cinit);
+  mma_k32(hi0, a[1], b0, b1, zero);
+  mma_k32(lo1, a[0], b2, b3, cinit);
+  mma_k32(hi1, a[1], b2, b3, zero);
+  uint32_t y0[4], y1[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    y0[e] = (uint32_t)lo0[e] + ((uint32_t)hi0[e] << 7);
+    y1[e] = (uint32_t)lo1[e] + ((uint32_t)hi1[e] << 7);
+  }
+  // D regs: [0] (block i, c=2q), [1] (i, c=2q+1), [2]/[3] block i+8; n-tile 1 is c+8
+  *(uint2*)(irow + w_e) = make_uint2(y0[0], y1[0]);
+  *(uint2*)(irow + w_o) = make_uint2(y0[1], y1[1]);
+  *(uint2*)(irow + w_e + 512) = make_uint2(y0[2], y1[2]);
+  *(uint2*)(irow + w_o + 512) = make_uint2(y0[3], y1[3]);
+}
+
+// Inverse stage B from int32 intermediates (the "wide" kernels): b[t] = the
+// two m16n8k32 B operand pairs of n-tile t (c = 8t .. 8t+7) for blocks m =
+// 0-7 and 8-15, each 32-bit word one stage-A sum S; the two K chunks
+// accumulate into one accumulator per limb.  Output as stage_m<true, kAdd>.
+template <bool kAdd>
+__device__ __forceinline__ void stage_m_inv_wide(const uint32_t (&a)[2][2][4], int32_t c_lo,
+                                                 int32_t c_hi, const uint32_t (&b)[2][4],
+                                                 uint8_t* row, uint32_t w_nat,
+                                                 const uint32_t (&add)[4]) {
+  const int32_t cinit[4] = {c_lo, c_lo, c_hi, c_hi};
+  const int32_t zero[4] = {0, 0, 0, 0};
+  int32_t lo0[4], hi0[4], lo1[4], hi1[4];
+  mma_k32(lo0, a[0][0], b[0][0], b[0][1], cinit);
+  mma_k32(hi0, a[1][0], b[0][0], b[0][1], zero);
+  mma_k32(lo1, a[0][0], b[1][0], b[1][1], cinit);
+  mma_k32(hi1, a[1][0], b[1][0], b[1][1], zero);
+  mma_k32(lo0, a[0][1], b[0][2], b[0][3], lo0);
+  mma_k32(hi0, a[1][1], b[0][2], b[0][3], hi0);
+  mma_k32(lo1, a[0][1], b[1][2], b[1][3], lo1);
+  mma_k32(hi1, a[1][1], b[1][2], b[1][3], hi1);
+  stage_m_out<true, kAdd>(lo0, hi0, lo1, hi1, row, 0, 0, w_nat, add);
 }
 
 // Forward stage 1 in single-limb form, for inputs in [-128, 127]: one data
@@ -146,6 +219,56 @@ __device__ __forceinline__ void stage_c(const uint32_t (&a)[2][2][2], const int3
     *(uint32_t*)(out + 32 * h) = pack2(e0, o0);
     *(uint32_t*)(out + kRowBytes + 32 * h) = pack2(e1, o1);
   }
+}
+
+// Forward stage 2 from int32 intermediates for blocks I, I+1 of 8
+// polynomials: r[4h .. 4h+3] = B operands of block I+h (even k0-15, even
+// k16-31, odd k0-15, odd k16-31), each 32-bit word one intermediate S.
+// Output as stage_c<false>: exact reduction, natural order, polynomials 2q
+// and 2q+1 of the n-tile.
+__device__ __forceinline__ void stage_c_wide(const uint32_t (&a)[2][2][4], const uint32_t (&r)[8],
+                                             uint8_t* out) {
+  const int32_t zero[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    int32_t de[4], dodd[4];
+    mma_k32(de, a[h][0], r[4 * h], r[4 * h + 1], zero);
+    mma_k32(dodd, a[h][1], r[4 * h + 2], r[4 * h + 3], zero);
+    const uint32_t e0 = red_exact((uint32_t)de[0] + ((uint32_t)de[2] << 7));
+    const uint32_t e1 = red_exact((uint32_t)de[1] + ((uint32_t)de[3] << 7));
+    const uint32_t o0 = red_exact((uint32_t)dodd[0] + ((uint32_t)dodd[2] << 7));
+    const uint32_t o1 = red_exact((uint32_t)dodd[1] + ((uint32_t)dodd[3] << 7));
+    *(uint32_t*)(out + 32 * h) = pack2(e0, o0);
+    *(uint32_t*)(out + kRowBytes + 32 * h) = pack2(e1, o1);
+  }
+}
+
+// Inverse stage A of blocks I, I+1 for 8 polynomials into int32
+// intermediates (the "wide" kernels).  x: biased, parity-split B operands as
+// stage_c<true>.  The sums S (< 2^24) of output c' = 2(lane/4) + s of blocks I
+// and I+1 go side by side (8 bytes) to polynomial 2q's row `rows` and 2q+1's
+// row rows + kWideRowBytes at offset off[s].  Row layout: [c][m], c at 64 c,
+// blocks m .. m+3 in the 16-byte chunk (m >> 2) ^ ((c >> 1) & 3) -- the xor
+// keeps stage B's ldmatrix rows on distinct banks.
+__device__ __forceinline__ void stage_c_inv_wide(const uint32_t (&a)[2][2][2],
+                                                 const int32_t (&ca)[2][2], const uint32_t (&x)[4],
+                                                 uint8_t* rows, const uint32_t (&off)[2]) {
+  uint32_t S[2][2][2];  // [parity][polynomial 2q + j][block I + h]
+#pragma unroll
+  for (int h = 0; h < 2; h++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      const int32_t c[4] = {ca[h][s], ca[h][s], 0, 0};
+      int32_t d[4];
+      mma_k16(d, a[h][s], x[2 * h + s], c);
+      S[s][0][h] = (uint32_t)d[0] + ((uint32_t)d[2] << 7);
+      S[s][1][h] = (uint32_t)d[1] + ((uint32_t)d[3] << 7);
+    }
+#pragma unroll
+  for (int s = 0; s < 2; s++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+      *(uint2*)(rows + j * kWideRowBytes + off[s]) = make_uint2(S[s][j][0], S[s][j][1]);
 }
 
 }  // namespace tk

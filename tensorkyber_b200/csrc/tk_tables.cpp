@@ -73,7 +73,12 @@ constexpr int64_t kInvScale = 512;
 
 uint8_t limb(int64_t v, int g) { return (uint8_t)(g ? (v >> 7) : (v & 127)); }
 
-int64_t byte_weighted(int64_t c, int byte) { return modq(byte ? c * 256 : c); }
+// c * 256^byte mod q: the constant that byte `byte` of a data word carries.
+int64_t byte_weighted(int64_t c, int byte) {
+  int64_t v = modq(c);
+  for (int j = 0; j < byte; j++) v = v * 256 % kQ;
+  return v;
+}
 
 }  // namespace
 
@@ -155,6 +160,15 @@ void build_fwd_frags(const Matrices& M, FwdFrags* F) {
             return limb(byte_weighted(M.m2[b][co][c], k & 1), r >> 3);
           },
           F->s2[b][s]);
+  for (int b = 0; b < 16; b++)
+    for (int s = 0; s < 2; s++)
+      pack_a_k32(
+          [&](int r, int k) {
+            const int co = 2 * (r & 7) + s;
+            const int c = 2 * fwd_slot_e(k >> 2) + s;
+            return limb(byte_weighted(M.m2[b][co][c], k & 3), r >> 3);
+          },
+          F->s2w[b][s]);
   // single-limb stage 1: two accumulator groups (lo / hi limb), rows 0..15
   // on the two A register halves of m16n8k16
   for (int g = 0; g < 2; g++)
@@ -195,6 +209,11 @@ void build_inv_frags(const Matrices& M, InvFrags* F) {
   for (int g = 0; g < 2; g++)
     pack_a_k32([&](int i, int k) { return limb(byte_weighted(M.minv[i][k >> 1], k & 1), g); },
                F->sb[g]);
+  for (int g = 0; g < 2; g++)
+    for (int j = 0; j < 2; j++)
+      pack_a_k32(
+          [&](int i, int k) { return limb(byte_weighted(M.minv[i][8 * j + (k >> 2)], k & 3), g); },
+          F->sbw[g][j]);
 }
 
 }  // namespace tk

@@ -58,6 +58,10 @@ constexpr uint32_t kBias10qPacked = 0x020A020Au;
 // Forward stage 2: per block b and parity s, A = 16x16 s8 (m16n8k16):
 // rows r<8 -> group 0, r>=8 -> group 1, output c' = 2*(r&7) + s; K k = 2*slot
 // + byte, slot j holds c = 2*e(j) + s with e(j) = (j>>1) + 4*(j&1).
+// Forward stage 2 from int32 intermediates (s2w, the "wide" kernels): per
+// block b and parity s, A = 16x32 s8 (m16n8k32); rows as s2; K k = 4*slot +
+// byte, the four bytes of a non-negative 32-bit stage-1 sum S (< 2^25), whose
+// byte j carries the constant times 256^j mod q; slot order as s2.
 // Forward stage 1, single-limb form (inputs in [-128, 127], one byte each):
 // A = 16x16 s8 (m16n8k16), rows i, K k' holds block m = pi(k') with
 // pi(4t + j) = 2t + j (j < 2), 8 + 2t + (j - 2) (j >= 2) -- the m order in
@@ -70,6 +74,7 @@ struct FwdFrags {
   uint32_t s2[16][2][32][2];
   uint32_t s1b[2][32][2];
   int32_t c1b[32][2];
+  uint32_t s2w[16][2][32][4];
 };
 
 // Inverse stage A: per block m and parity s, A = 16x16 s8; rows as in forward
@@ -77,12 +82,18 @@ struct FwdFrags {
 // stage-2 slot order (slot j holds input c = 2*e(j) + s).  Inputs are biased
 // with x ^ 0x8000; ca holds the group-0 accumulator init of row lane/4, the
 // (-32768 * rowsum) mod q correction.
-// Inverse stage B: A = 16x32 s8, rows i, K k = 2*m + byte; no correction.  The
-// kernel adds (q-1)/2 in the group-0 accumulator init to centre the output.
+// Inverse stage B: A = 16x32 s8, rows i, K k = 2*m + byte; no correction (the
+// kernels centre the output in the reduction, red_centred).
+// Inverse stage B from int32 intermediates (sbw, the "wide" kernels): per limb
+// g and K chunk j (blocks m = 8j .. 8j+7), A = 16x32 s8, rows i, K k =
+// 4*(m - 8j) + byte, the four bytes of a non-negative stage-A sum (< 2^24),
+// byte t carrying the constant times 256^t mod q; the two chunks accumulate
+// into one accumulator.
 struct InvFrags {
   uint32_t sa[16][2][32][2];
   int32_t ca[16][2][32];
   uint32_t sb[2][32][4];
+  uint32_t sbw[2][2][32][4];
 };
 
 // Logical matrices (canonical residues in [0, q)).

@@ -52,6 +52,9 @@ class FwdModel:
         s2 = w[320:2368].reshape(16, 2, 32, 2)
         s1b = w[2368:2496].reshape(2, 32, 2)
         c1b = w[2496:2560].view(np.int32).reshape(32, 2)
+        s2w = w[2560:6656].reshape(16, 2, 32, 4)
+        # stage 2 from int32 intermediates: K = 4 * slot + byte
+        self.A2w = [[unpack_k32(s2w[b][s]) for s in range(2)] for b in range(16)]
         # single-limb stage 1: A columns k' hold block m = pi(k')
         self.A1b = [unpack_k16(s1b[g]) for g in range(2)]
         self.corr_b = np.zeros(16, dtype=np.int64)
@@ -68,9 +71,11 @@ class FwdModel:
         self.corr = corr
         self.A2 = [[unpack_k16(s2[b][s]) for s in range(2)] for b in range(16)]
 
-    def __call__(self, x: np.ndarray, single_limb: bool = False) -> np.ndarray:
+    def __call__(self, x: np.ndarray, single_limb: bool = False, wide: bool = False) -> np.ndarray:
         """single_limb: the stage-1 form for inputs in [-128, 127] (one data
-        byte x + 128 per coefficient, K in the pi order of the fragments)."""
+        byte x + 128 per coefficient, K in the pi order of the fragments).
+        wide: the stage-1 sums stay unreduced int32 and stage 2 reads their
+        four bytes (the int32-intermediate kernels)."""
         x = np.asarray(x, dtype=np.int16).reshape(-1, 256)
         P = x.shape[0]
         if single_limb:
@@ -86,15 +91,22 @@ class FwdModel:
             D1 = np.einsum("ik,pkc->pic", self.A1[1], X)
         S = D0 + 128 * D1
         assert S.min() >= 0 and S.max() < (1 << 25), (S.min(), S.max())
-        mid = S - ((S * BAR_LAZY) >> 32) * Q                                 # [p][i][c]
-        assert mid.min() >= 0 and mid.max() < Q + 8
+        if wide:
+            mid = S
+        else:
+            mid = S - ((S * BAR_LAZY) >> 32) * Q                             # [p][i][c]
+            assert mid.min() >= 0 and mid.max() < Q + 8
         out = np.zeros((P, 256), dtype=np.int64)
         for b in range(16):
             for s in range(2):
                 cols = [2 * fwd_slot_e(j) + s for j in range(8)]
                 v = mid[:, b, cols]                                          # [p][slot]
-                B = np.stack([v & 255, v >> 8], axis=2).reshape(P, 16)       # [p][k]
-                D = B @ self.A2[b][s].T                                       # [p][row]
+                if wide:
+                    B = np.stack([(v >> (8 * t)) & 255 for t in range(4)], axis=2).reshape(P, 32)
+                    D = B @ self.A2w[b][s].T
+                else:
+                    B = np.stack([v & 255, v >> 8], axis=2).reshape(P, 16)   # [p][k]
+                    D = B @ self.A2[b][s].T                                   # [p][row]
                 S2 = D[:, :8] + 128 * D[:, 8:]
                 assert S2.min() >= 0 and S2.max() < (1 << 26)
                 r = S2 - ((S2 * BAR_EXACT) >> 38) * Q
@@ -109,7 +121,9 @@ class InvModel:
         w = np.asarray(words, dtype=np.uint32)
         sa = w[:2048].reshape(16, 2, 32, 2)
         ca = w[2048:3072].view(np.int32).reshape(16, 2, 32)
-        sb = w[3072:].reshape(2, 32, 4)
+        sb = w[3072:3328].reshape(2, 32, 4)
+        sbw = w[3328:3840].reshape(2, 2, 32, 4)
+        self.ABw = [[unpack_k32(sbw[g][j]) for j in range(2)] for g in range(2)]
         self.AA = [[unpack_k16(sa[b][s]) for s in range(2)] for b in range(16)]
         self.corr = np.zeros((16, 2, 8), dtype=np.int64)          # [block][parity][row a]
         for b in range(16):
@@ -118,7 +132,9 @@ class InvModel:
                     self.corr[b, s, lane // 4] = ca[b][s][lane]
         self.AB = [unpack_k32(sb[g]) for g in range(2)]
 
-    def __call__(self, x: np.ndarray) -> np.ndarray:
+    def __call__(self, x: np.ndarray, wide: bool = False) -> np.ndarray:
+        """wide: the stage-A sums stay unreduced int32 and stage B reads their
+        four bytes in two K chunks of 8 blocks (the int32-intermediate kernels)."""
         x = np.asarray(x, dtype=np.int16).reshape(-1, 256)
         P = x.shape[0]
         u = x.view(np.uint16).astype(np.int64) ^ 0x8000                   # x + 32768
@@ -129,16 +145,26 @@ class InvModel:
                 B = np.stack([v & 255, v >> 8], axis=2).reshape(P, 16)
                 D = B @ self.AA[b][s].T
                 S = D[:, :8] + self.corr[b, s][None, :] + 128 * D[:, 8:]
-                assert S.min() >= 0 and S.max() < (1 << 25)
-                r = S - ((S * BAR_LAZY) >> 32) * Q
+                assert S.min() >= 0 and S.max() < (1 << (24 if wide else 25))
+                r = S if wide else S - ((S * BAR_LAZY) >> 32) * Q
                 for a in range(8):
                     mid[:, 16 * b + 2 * a + s] = r[:, a]
-        m = mid.reshape(P, 16, 16)
-        X = np.stack([m & 255, m >> 8], axis=2).reshape(P, 32, 16)
-        D0 = 1664 + np.einsum("ik,pkc->pic", self.AB[0], X)
-        D1 = np.einsum("ik,pkc->pic", self.AB[1], X)
+        m = mid.reshape(P, 16, 16)                                        # [p][m][c]
+        if wide:
+            D0 = 0
+            D1 = 0
+            for j in range(2):
+                X = np.stack([(m[:, 8 * j:8 * j + 8, :] >> (8 * t)) & 255 for t in range(4)],
+                             axis=2).reshape(P, 32, 16)                  # [p][4 m' + byte][c]
+                D0 = D0 + np.einsum("ik,pkc->pic", self.ABw[0][j], X)
+                D1 = D1 + np.einsum("ik,pkc->pic", self.ABw[1][j], X)
+        else:
+            X = np.stack([m & 255, m >> 8], axis=2).reshape(P, 32, 16)
+            D0 = np.einsum("ik,pkc->pic", self.AB[0], X)
+            D1 = np.einsum("ik,pkc->pic", self.AB[1], X)
         S = D0 + 128 * D1
-        assert S.min() >= 0 and S.max() < (1 << 26)
-        r = S - ((S * BAR_EXACT) >> 38) * Q - 1664
+        # centred reduction: floor((S + 1664) / q) from the exact multiplier
+        assert S.min() >= 0 and S.max() + 1664 < (1 << 26)
+        r = S - (((S + 1664) * BAR_EXACT) >> 38) * Q
         assert r.min() >= -1664 and r.max() <= 1664
         return r.reshape(P, 256).astype(np.int16)

@@ -163,3 +163,19 @@ def test_matvec_full_mixed_workload_sample(tk, cuda, oracle, mode):
         pick = rng(k).choice(A.shape[0], 300, replace=False)
         assert (canon(out[pick]) == canon(oracle_out(oracle, k, A[pick], s[pick], e[pick]))).all()
     assert tk.device_status(0) == 0
+
+
+@pytest.mark.parametrize("variant", range(4))
+def test_matvec_pipeline_every_variant(tk, cuda, oracle, variant):
+    """The pipeline's forward and inverse-with-addend launches in each batch
+    kernel variant (one batch, so the single-batch kernels run)."""
+    A, s, e = make_jobs(40 + variant, 3, 150)
+    tk.set_option(tk.OPT_MATVEC_MODE, 0)
+    try:
+        tk.set_variant(tk.FORWARD, variant)
+        tk.set_variant(tk.INVERSE, variant)
+        (out,) = run(tk, cuda, [(3, A, s, e)])
+    finally:
+        tk.set_variant(tk.FORWARD, -1)
+        tk.set_variant(tk.INVERSE, -1)
+    assert (canon(out) == canon(oracle_out(oracle, 3, A, s, e))).all()

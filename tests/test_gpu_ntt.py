@@ -57,9 +57,12 @@ def test_uniform_sizes(tk, cuda, oracle, n):
     check_inv(gpu_inv(tk, cuda, x), oracle.invntt(x))
 
 
-@pytest.mark.parametrize("variant", range(3))
+NVARIANTS = 4
+
+
+@pytest.mark.parametrize("variant", range(NVARIANTS))
 def test_every_variant(tk, cuda, oracle, variant):
-    assert tk.variant_count() == 3
+    assert tk.variant_count() == NVARIANTS
     try:
         tk.set_variant(tk.FORWARD, variant)
         tk.set_variant(tk.INVERSE, variant)
@@ -269,7 +272,7 @@ def test_autotune_small_range(tk, cuda, oracle, tmp_path):
         tk.autotune_reset()
 
 
-@pytest.mark.parametrize("variant", range(3))
+@pytest.mark.parametrize("variant", range(NVARIANTS))
 def test_every_variant_many_tiles_per_cta(tk, cuda, oracle, variant):
     """300,000 polynomials: every CTA walks tens of tiles, so each slot of
     every variant's ring is refilled many times.  Outputs must equal the

@@ -51,28 +51,30 @@ def test_logical_matrices_compose_to_oracle(mats, oracle):
     assert (apply_inv(mats, x) == canon(oracle.invntt(x))).all()
 
 
+@pytest.mark.parametrize("wide", [False, True], ids=["int16-mid", "int32-mid"])
 @pytest.mark.parametrize("lo,hi", [(0, Q), (-3, 4), (-32768, 32768)])
-def test_kernel_arithmetic_model(tk, oracle, lo, hi):
+def test_kernel_arithmetic_model(tk, oracle, lo, hi, wide):
     fw = KM.FwdModel(tk.get_table(4))
     iv = KM.InvModel(tk.get_table(5))
     x = rng(hi).integers(lo, hi, size=(200, 256)).astype(np.int16)
     ref_in = canon(x).astype(np.int16)        # the oracle overflows outside |x| < 9471
-    f = fw(x)
+    f = fw(x, wide=wide)
     assert f.min() >= 0 and f.max() < Q
     assert (f == canon(oracle.ntt(ref_in))).all()
-    v = iv(x)
+    v = iv(x, wide=wide)
     assert v.min() >= -(Q // 2) and v.max() <= Q // 2
     assert (canon(v) == canon(oracle.invntt(ref_in))).all()
 
 
-def test_kernel_model_extreme_rows(tk, oracle):
+@pytest.mark.parametrize("wide", [False, True], ids=["int16-mid", "int32-mid"])
+def test_kernel_model_extreme_rows(tk, oracle, wide):
     fw = KM.FwdModel(tk.get_table(4))
     iv = KM.InvModel(tk.get_table(5))
     x = np.array([[-32768] * 256, [32767] * 256, [Q - 1] * 256, [0] * 256,
                   np.tile([32767, -32768], 128)], dtype=np.int16)
     ref_in = canon(x).astype(np.int16)
-    assert (fw(x) == canon(oracle.ntt(ref_in))).all()
-    assert (canon(iv(x)) == canon(oracle.invntt(ref_in))).all()
+    assert (fw(x, wide=wide) == canon(oracle.ntt(ref_in))).all()
+    assert (canon(iv(x, wide=wide)) == canon(oracle.invntt(ref_in))).all()
 
 
 @pytest.mark.parametrize("lo,hi", [(-128, 128), (-3, 4), (-1, 2)])
