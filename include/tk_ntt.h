@@ -197,9 +197,11 @@ int tk_server_destroy(tk_server *srv, double timeout_s);
  * TK_OPT_MATVEC_MODE: TK_MATVEC_PIPELINE (NTT, basemul-accumulate and iNTT+e
  * as three stream-ordered kernels per chunk) or TK_MATVEC_FUSED (one kernel,
  * one warp per job: every intermediate stays in shared memory).
- * TK_OPT_HOST_CHUNK_POLYS: polynomials per copy-in / transform / copy-out
- * chunk of tk_ntt_host / tk_invntt_host (1 .. 32768, the default; smaller chunks
- * are slower on a B200 host link: the path runs at the link rate). */
+ * TK_OPT_HOST_CHUNK_POLYS: largest number of polynomials per copy-in /
+ * transform / copy-out chunk of tk_ntt_host / tk_invntt_host (1 .. 32768, the
+ * default; smaller chunks are slower on a B200 host link: the path runs at the
+ * link rate).  The first chunks of a call grow from 4096 polynomials to it and
+ * the last ones shrink back, so the copies that cannot overlap stay short. */
 #define TK_OPT_MATVEC_CHUNK_POLYS 1
 #define TK_OPT_MATVEC_MODE 2
 #define TK_OPT_HOST_CHUNK_POLYS 3

@@ -208,9 +208,23 @@ int run_device(bool inverse, const int16_t* in, int16_t* out, size_t npoly, cuda
   return TK_SUCCESS;
 }
 
-// Host path: chunks of stage_polys polynomials rotate through three device
-// buffers and three streams, so the H2D copy of chunk c+1, the kernel of chunk
-// c and the D2H copy of chunk c-1 overlap.
+// Host path: chunks of at most stage_polys polynomials rotate through
+// kHostStages device buffers and streams, so the H2D copy of chunk c+1, the
+// kernel of chunk c and the D2H copy of chunk c-1 overlap, and an upload
+// waits only for the download kHostStages chunks back.  The first chunks grow
+// from kHostRampPolys and the last ones shrink to it: the first upload and the
+// last download run with nothing beside them, so they are kept short.
+constexpr size_t kHostRampPolys = 4096;
+constexpr int kHostStages = 3;  // 4 measured the same
+size_t host_chunk_size(int c, size_t remaining, size_t chunk) {
+  size_t n = chunk;
+  if (c < 16 && (kHostRampPolys << c) < n) n = kHostRampPolys << c;
+  const size_t half = (remaining + 1) / 2;
+  const size_t tail = half > kHostRampPolys ? half : kHostRampPolys;
+  if (tail < n) n = tail;
+  if (remaining - n < kHostRampPolys && remaining <= chunk) n = remaining;  // no sliver
+  return n < remaining ? n : remaining;
+}
 int run_host(bool inverse, int16_t* polys, size_t npoly) {
   t_err[0] = 0;
   if (npoly == 0) return TK_SUCCESS;
@@ -233,11 +247,11 @@ int run_host(bool inverse, int16_t* polys, size_t npoly) {
   cudaError_t e;
   if (!S.stage[0]) {
     S.stage_polys = kHostStagePolys;
-    for (int i = 0; i < 3; i++) {
+    for (int i = 0; i < kHostStages; i++) {
       if ((e = cudaMalloc(&S.stage[i], S.stage_polys * 512u)) != cudaSuccess ||
           (e = cudaStreamCreateWithFlags(&S.streams[i], cudaStreamNonBlocking)) != cudaSuccess) {
         set_err("host-path staging set-up", e);
-        for (int j = 0; j < 3; j++) {
+        for (int j = 0; j < kHostStages; j++) {
           if (S.stage[j]) cudaFree(S.stage[j]);
           if (S.streams[j]) cudaStreamDestroy(S.streams[j]);
           S.stage[j] = nullptr;
@@ -253,9 +267,9 @@ int run_host(bool inverse, int16_t* polys, size_t npoly) {
   int c = 0;
   e = cudaSuccess;
   while (done < npoly && e == cudaSuccess) {
-    const size_t n = (npoly - done < chunk) ? npoly - done : chunk;
-    cudaStream_t st = S.streams[c % 3];
-    int16_t* buf = S.stage[c % 3];
+    const size_t n = host_chunk_size(c, npoly - done, chunk);
+    cudaStream_t st = S.streams[c % kHostStages];
+    int16_t* buf = S.stage[c % kHostStages];
     e = cudaMemcpyAsync(buf, polys + done * 256, n * 512u, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
       e = tk::launch_mma(inverse, choose_variant(inverse, n), buf, buf, (long long)n, *info, st);
@@ -264,7 +278,7 @@ int run_host(bool inverse, int16_t* polys, size_t npoly) {
     done += n;
     c++;
   }
-  for (int i = 0; i < 3; i++) {
+  for (int i = 0; i < kHostStages; i++) {
     cudaError_t e2 = cudaStreamSynchronize(S.streams[i]);
     if (e == cudaSuccess) e = e2;
   }
