@@ -54,8 +54,10 @@ constexpr int kMaxSegs = 4;  // batches per kernel launch
 // Transforms every segment, packing up to kMaxSegs of them (pieces of at
 // most kMaxLaunchPolys) into each kernel launch, so several small batches
 // fill the GPU like one large one.  A launch of one piece uses the given
-// variant's single-batch kernel; a launch of several uses variant 0's shape.  A segment with an addend selects the
-// inverse-with-addend kernel for its launch (segments without one add nothing).
+// variant's single-batch kernel; a launch of several uses the default
+// variants' shapes (forward 3, inverse 0).  A segment with an addend selects
+// the inverse-with-addend kernel for its launch (segments without one add
+// nothing).
 cudaError_t launch_mma_segs(bool inverse, int variant, const Seg* segs, int nseg,
                             const DeviceInfo& info, cudaStream_t stream);
 

@@ -380,7 +380,8 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn, kWide>::kMinBlocks)
   constexpr bool kMulti = std::is_same<Param, SegMaps>::value;
   static_assert(!kInverse || kIn == kInInt16, "input forms are forward only");
   static_assert(kInverse || !kAdd, "the addend is an inverse option");
-  static_assert(!kWide || (kIn == kInInt16 && !kMulti), "wide: int16 input, one segment");
+  static_assert(!kWide || (kIn == kInInt16 && !(kMulti && kInverse)),
+                "wide: int16 input; the inverse with one segment");
   using C = Cfg<W, S, kIn, kWide>;
   extern __shared__ __align__(128) uint8_t smem[];
   const int tid = threadIdx.x;
@@ -693,11 +694,11 @@ static const Variant kAddVariants[kNumMmaVariants] = {
     make_variant<true, 4, 3, kInInt16, true>(), make_variant<true, 8, 3, kInInt16, true>(),
     make_variant<true, 4, 2, kInInt16, true>(),
     make_variant<true, 4, 2, kInInt16, true, OneSeg, true>()};
-// Launches over several segments (variant 0's shape): forward, inverse,
-// inverse with addend.  Kept apart so that single-batch launches carry none of
-// the segment lookup.
+// Launches over several segments (the default variants' shapes: forward 3,
+// inverse 0): forward, inverse, inverse with addend.  Kept apart so that
+// single-batch launches carry none of the segment lookup.
 static const Variant kMultiVariants[3] = {
-    make_variant<false, 4, 3, kInInt16, false, SegMaps>(),
+    make_variant<false, 4, 2, kInInt16, false, SegMaps, true>(),
     make_variant<true, 4, 3, kInInt16, false, SegMaps>(),
     make_variant<true, 4, 3, kInInt16, true, SegMaps>()};
 
