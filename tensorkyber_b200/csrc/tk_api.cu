@@ -58,8 +58,9 @@ const char* const kVariantNames[tk::kNumMmaVariants] = {
 };
 
 // Autotuned choice per direction and size bucket floor(log2(npoly)); -1 =
-// not tuned: variant 3 for the forward and variant 0 for the inverse, the
-// fastest shapes measured at 2^18 and 2^20 polynomials.
+// not tuned: variant 3 for the forward; for the inverse variant 0 below 2^19
+// polynomials and variant 2 from there (the fastest shapes measured at 2^18
+// and 2^20).
 constexpr int kBuckets = 33;
 std::atomic<int> g_tuned[2][kBuckets];
 struct TunedInit {
@@ -79,7 +80,8 @@ int choose_variant(bool inverse, size_t npoly) {
   const int f = g_forced[inverse ? 1 : 0].load(std::memory_order_relaxed);
   if (f >= 0) return f;
   const int t = g_tuned[inverse ? 1 : 0][size_bucket(npoly)].load(std::memory_order_relaxed);
-  return t >= 0 ? t : (inverse ? 0 : 3);
+  if (t >= 0) return t;
+  return inverse ? (npoly >= ((size_t)1 << 19) ? 2 : 0) : 3;
 }
 
 void set_err(const char* what, cudaError_t e) {

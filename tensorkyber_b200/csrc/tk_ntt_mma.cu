@@ -229,8 +229,8 @@ __device__ __forceinline__ void block_stage_inv_wide(uint32_t slot, int blk0, ui
 template <bool kAdd>
 __device__ __forceinline__ void poly_stage_inv_wide(uint32_t irow0, uint8_t* minep,
                                                     const uint32_t (&lb)[2],
-                                                    const uint32_t (&a)[2][2][4], int32_t cm_lo,
-                                                    int32_t cm_hi, uint32_t w_nat,
+                                                    const uint32_t (&a)[2][2][4],
+                                                    const int32_t (&cb)[2][4], uint32_t w_nat,
                                                     const uint32_t* addend, int poly0, int npoly,
                                                     uint32_t add_off) {
   auto load_add = [&](int p, uint32_t (&e)[4]) {
@@ -258,7 +258,7 @@ __device__ __forceinline__ void poly_stage_inv_wide(uint32_t irow0, uint8_t* min
       ldsm_x4(nx + lb[1], n[1][0], n[1][1], n[1][2], n[1][3]);
       load_add(p + 1, en);
     }
-    stage_m_inv_wide<kAdd>(a, cm_lo, cm_hi, b, minep + p * kRowBytes, w_nat, e);
+    stage_m_inv_wide<kAdd>(a, cb, b, minep + p * kRowBytes, w_nat, e);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       b[0][j] = n[0][j];
@@ -275,7 +275,8 @@ __device__ __forceinline__ void poly_stage_inv_wide(uint32_t irow0, uint8_t* min
 template <bool kInverse, bool kAdd = false>
 __device__ __forceinline__ void poly_stage(uint32_t mine, uint8_t* minep, uint32_t ldt_off,
                                            const uint32_t (&am)[2][4], int32_t cm_lo,
-                                           int32_t cm_hi, uint32_t w_even, uint32_t w_odd,
+                                           int32_t cm_hi, const int32_t (&cb)[2][4],
+                                           uint32_t w_even, uint32_t w_odd,
                                            uint32_t w_nat, const uint32_t* addend, int poly0,
                                            int npoly, uint32_t add_off) {
   auto load_add = [&](int p, uint32_t (&e)[4]) {
@@ -301,7 +302,7 @@ __device__ __forceinline__ void poly_stage(uint32_t mine, uint8_t* minep, uint32
       load_add(p + 1, en);
     }
     if (kInverse)
-      stage_m<true, kAdd>(am, cm_lo, cm_hi, b[0], b[1], b[2], b[3], minep + p * kRowBytes, 0, 0,
+      stage_m_q<true, kAdd>(am, cb[0], cb[1], b[0], b[1], b[2], b[3], minep + p * kRowBytes, 0, 0,
                     w_nat, e);
     else  // x ^ 0x8000 bias; the 32768 * rowsum term is cancelled by cm_lo/cm_hi
       stage_m<false>(am, cm_lo, cm_hi, b[0] ^ 0x80008000u, b[1] ^ 0x80008000u,
@@ -406,7 +407,14 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn, kWide>::kMinBlocks)
   int32_t cm_lo, cm_hi;                    // its accumulator init
   constexpr int kAW = kWide && !kInverse ? 4 : 2;  // A registers (k16, or k32 wide forward)
   uint32_t ac[C::kPairsPerWarp][2][2][kAW];  // block-wise stage, per (pair, block, parity)
-  int32_t cc[C::kPairsPerWarp][2][2];      // its group-0 accumulator init
+  // block-wise stage accumulator init: zero (the inverse's stage-A bias
+  // offset is cancelled by stage B's init cb instead)
+  int32_t cc[C::kPairsPerWarp][2][2];
+  int32_t cb[2][4];  // inverse stage B: group-0 init per n-tile (InvFrags::cbz)
+#pragma unroll
+  for (int t = 0; t < 2; t++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) cb[t][j] = kInverse ? g_inv.cbz[lane][t][j] : 0;
   const int blk0 = C::kBlocksPerWarp * warp;
 #pragma unroll
   for (int g = 0; g < 2; g++)
@@ -446,7 +454,7 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn, kWide>::kMinBlocks)
           ac[p][h][s][j] = (kWide && !kInverse) ? g_fwd.s2w[b][s][lane][j]
                            : kInverse ? g_inv.sa[b][s][lane][j & 1]
                                       : g_fwd.s2[b][s][lane][j & 1];
-        cc[p][h][s] = kInverse ? g_inv.ca[b][s][lane] : 0;
+        cc[p][h][s] = 0;
       }
 
   if (tid == 0) {
@@ -600,7 +608,7 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn, kWide>::kMinBlocks)
       block_stage_inv_wide<W>(slot, blk0, ldc_off, interp, ia_row, ia, ac, cc);
       cta_sync_named();
       const int unit = u_begin + k * W + warp;
-      poly_stage_inv_wide<kAdd>(inter + 8 * warp * kWideRowBytes, minep, lb, amw, cm_lo, cm_hi,
+      poly_stage_inv_wide<kAdd>(inter + 8 * warp * kWideRowBytes, minep, lb, amw, cb,
                                 w_nat, kAdd ? seg_addend(0) : nullptr, 8 * unit,
                                 kAdd ? seg_npoly(0) : 0, 8u * g8 + q4);
       fence_proxy_async_smem();
@@ -627,7 +635,7 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn, kWide>::kMinBlocks)
       issue_store(k, slot_i);
     } else if (!kInverse) {
       if (kIn == kInInt16)
-        poly_stage<false>(mine, minep, ldt_off, am, cm_lo, cm_hi, w_even, w_odd, 0, nullptr, 0, 0,
+        poly_stage<false>(mine, minep, ldt_off, am, cm_lo, cm_hi, cb, w_even, w_odd, 0, nullptr, 0, 0,
                           0);
       else {
         // a warp without a unit in this tile computes on stale rows (its
@@ -648,7 +656,7 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn, kWide>::kMinBlocks)
       cta_sync_named();
       const int unit = u_begin + k * W + warp;
       const int sg = kAdd ? seg_of(unit) : 0;
-      poly_stage<true, kAdd>(mine, minep, ldt_off, am, cm_lo, cm_hi, 0, 0, w_nat,
+      poly_stage<true, kAdd>(mine, minep, ldt_off, am, cm_lo, cm_hi, cb, 0, 0, w_nat,
                              kAdd ? seg_addend(sg) : nullptr,
                              8 * (unit - seg_first(sg)), kAdd ? seg_npoly(sg) : 0,
                              8u * g8 + q4);

@@ -24,19 +24,29 @@ __device__ __forceinline__ void stage_m_out(const int32_t (&lo0)[4], const int32
 // operands (ldmatrix.trans of the natural-order row) are b0..b3.  Inverse
 // with kAdd: the addend pairs `add` are added to the output (int16
 // wrap-around); without it `add` is ignored.
+// c0 / c1: the group-0 accumulator init of n-tiles 0 and 1 (D register order).
+template <bool kInverse, bool kAdd = false>
+__device__ __forceinline__ void stage_m_q(const uint32_t (&a)[2][4], const int32_t (&c0)[4],
+                                          const int32_t (&c1)[4], uint32_t b0, uint32_t b1,
+                                          uint32_t b2, uint32_t b3, uint8_t* row, uint32_t w_even,
+                                          uint32_t w_odd, uint32_t w_nat,
+                                          const uint32_t (&add)[4]) {
+  const int32_t zero[4] = {0, 0, 0, 0};
+  int32_t lo0[4], hi0[4], lo1[4], hi1[4];
+  mma_k32(lo0, a[0], b0, b1, c0);
+  mma_k32(hi0, a[1], b0, b1, zero);
+  mma_k32(lo1, a[0], b2, b3, c1);
+  mma_k32(hi1, a[1], b2, b3, zero);
+  stage_m_out<kInverse, kAdd>(lo0, hi0, lo1, hi1, row, w_even, w_odd, w_nat, add);
+}
+// The same with one init per row half (rows lane/4 and lane/4 + 8).
 template <bool kInverse, bool kAdd = false>
 __device__ __forceinline__ void stage_m(const uint32_t (&a)[2][4], int32_t c_lo, int32_t c_hi,
                                         uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3,
                                         uint8_t* row, uint32_t w_even, uint32_t w_odd,
                                         uint32_t w_nat, const uint32_t (&add)[4]) {
   const int32_t cinit[4] = {c_lo, c_lo, c_hi, c_hi};
-  const int32_t zero[4] = {0, 0, 0, 0};
-  int32_t lo0[4], hi0[4], lo1[4], hi1[4];
-  mma_k32(lo0, a[0], b0, b1, cinit);
-  mma_k32(hi0, a[1], b0, b1, zero);
-  mma_k32(lo1, a[0], b2, b3, cinit);
-  mma_k32(hi1, a[1], b2, b3, zero);
-  stage_m_out<kInverse, kAdd>(lo0, hi0, lo1, hi1, row, w_even, w_odd, w_nat, add);
+  stage_m_q<kInverse, kAdd>(a, cinit, cinit, b0, b1, b2, b3, row, w_even, w_odd, w_nat, add);
 }
 
 // Epilogue of the stage over m from its accumulators (lo / hi limb, n-tiles 0
@@ -120,16 +130,15 @@ __device__ __forceinline__ void stage_m_wide(const uint32_t (&a)[2][4], int32_t 
 // 0-7 and 8-15, each 32-bit word one stage-A sum S; the two K chunks
 // accumulate into one accumulator per limb.  Output as stage_m<true, kAdd>.
 template <bool kAdd>
-__device__ __forceinline__ void stage_m_inv_wide(const uint32_t (&a)[2][2][4], int32_t c_lo,
-                                                 int32_t c_hi, const uint32_t (&b)[2][4],
-                                                 uint8_t* row, uint32_t w_nat,
-                                                 const uint32_t (&add)[4]) {
-  const int32_t cinit[4] = {c_lo, c_lo, c_hi, c_hi};
+__device__ __forceinline__ void stage_m_inv_wide(const uint32_t (&a)[2][2][4],
+                                                 const int32_t (&c)[2][4],
+                                                 const uint32_t (&b)[2][4], uint8_t* row,
+                                                 uint32_t w_nat, const uint32_t (&add)[4]) {
   const int32_t zero[4] = {0, 0, 0, 0};
   int32_t lo0[4], hi0[4], lo1[4], hi1[4];
-  mma_k32(lo0, a[0][0], b[0][0], b[0][1], cinit);
+  mma_k32(lo0, a[0][0], b[0][0], b[0][1], c[0]);
   mma_k32(hi0, a[1][0], b[0][0], b[0][1], zero);
-  mma_k32(lo1, a[0][0], b[1][0], b[1][1], cinit);
+  mma_k32(lo1, a[0][0], b[1][0], b[1][1], c[1]);
   mma_k32(hi1, a[1][0], b[1][0], b[1][1], zero);
   mma_k32(lo0, a[0][1], b[0][2], b[0][3], lo0);
   mma_k32(hi0, a[1][1], b[0][2], b[0][3], hi0);

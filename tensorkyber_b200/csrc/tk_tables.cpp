@@ -214,6 +214,27 @@ void build_inv_frags(const Matrices& M, InvFrags* F) {
       pack_a_k32(
           [&](int i, int k) { return limb(byte_weighted(M.minv[i][8 * j + (k >> 2)], k & 3), g); },
           F->sbw[g][j]);
+  // stage B init that cancels stage A's bias offset 32768 * rowsum(MA[m][c])
+  int64_t off[16][16];
+  for (int m = 0; m < 16; m++)
+    for (int c = 0; c < 16; c++) {
+      int64_t rs = 0;
+      for (int j = 0; j < 16; j++) rs += M.ma[m][c][j];
+      off[m][c] = modq(32768 * rs);
+    }
+  auto init = [&](int i, int c) {
+    int64_t v = 0;
+    for (int m = 0; m < 16; m++) v += (int64_t)M.minv[i][m] * off[m][c];
+    return (int32_t)modq(-v);
+  };
+  for (int lane = 0; lane < 32; lane++)
+    for (int t = 0; t < 2; t++) {
+      const int i = lane >> 2, c = 8 * t + 2 * (lane & 3);
+      F->cbz[lane][t][0] = init(i, c);
+      F->cbz[lane][t][1] = init(i, c + 1);
+      F->cbz[lane][t][2] = init(i + 8, c);
+      F->cbz[lane][t][3] = init(i + 8, c + 1);
+    }
 }
 
 }  // namespace tk

@@ -81,7 +81,8 @@ struct FwdFrags {
 // stage 2 (output c' = 2*(r&7) + s); K k = 2*slot + byte with the forward
 // stage-2 slot order (slot j holds input c = 2*e(j) + s).  Inputs are biased
 // with x ^ 0x8000; ca holds the group-0 accumulator init of row lane/4, the
-// (-32768 * rowsum) mod q correction.
+// (-32768 * rowsum) mod q correction (the fused matrix-vector kernel's; the
+// batch kernels cancel the bias in stage B instead, cbz below).
 // Inverse stage B: A = 16x32 s8, rows i, K k = 2*m + byte; no correction (the
 // kernels centre the output in the reduction, red_centred).
 // Inverse stage B from int32 intermediates (sbw, the "wide" kernels): per limb
@@ -89,11 +90,17 @@ struct FwdFrags {
 // 4*(m - 8j) + byte, the four bytes of a non-negative stage-A sum (< 2^24),
 // byte t carrying the constant times 256^t mod q; the two chunks accumulate
 // into one accumulator.
+// cbz: stage B's group-0 accumulator init when stage A runs without ca
+// (the batch kernels): stage A's output then carries 32768 * rowsum(MA[m][c])
+// mod q too, and stage B, linear, maps that to the constant Minv * offset;
+// cbz[lane][t] = -(Minv * offset) mod q at the lane's D registers of n-tile t
+// (rows lane/4 and lane/4 + 8, columns c = 8t + 2(lane%4) and c + 1).
 struct InvFrags {
   uint32_t sa[16][2][32][2];
   int32_t ca[16][2][32];
   uint32_t sb[2][32][4];
   uint32_t sbw[2][2][32][4];
+  int32_t cbz[32][2][4];
 };
 
 // Logical matrices (canonical residues in [0, q)).

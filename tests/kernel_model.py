@@ -122,6 +122,15 @@ class InvModel:
         sa = w[:2048].reshape(16, 2, 32, 2)
         ca = w[2048:3072].view(np.int32).reshape(16, 2, 32)
         sb = w[3072:3328].reshape(2, 32, 4)
+        cbz = w[3840:4096].view(np.int32).reshape(32, 2, 4)
+        # stage-B init [i][c] when stage A runs without its bias correction
+        self.binit = np.zeros((16, 16), dtype=np.int64)
+        for lane in range(32):
+            for t in range(2):
+                c = 8 * t + 2 * (lane % 4)
+                i = lane // 4
+                self.binit[i, c], self.binit[i, c + 1] = cbz[lane][t][0], cbz[lane][t][1]
+                self.binit[i + 8, c], self.binit[i + 8, c + 1] = cbz[lane][t][2], cbz[lane][t][3]
         sbw = w[3328:3840].reshape(2, 2, 32, 4)
         self.ABw = [[unpack_k32(sbw[g][j]) for j in range(2)] for g in range(2)]
         self.AA = [[unpack_k16(sa[b][s]) for s in range(2)] for b in range(16)]
@@ -132,9 +141,11 @@ class InvModel:
                     self.corr[b, s, lane // 4] = ca[b][s][lane]
         self.AB = [unpack_k32(sb[g]) for g in range(2)]
 
-    def __call__(self, x: np.ndarray, wide: bool = False) -> np.ndarray:
+    def __call__(self, x: np.ndarray, wide: bool = False, fold: bool = False) -> np.ndarray:
         """wide: the stage-A sums stay unreduced int32 and stage B reads their
-        four bytes in two K chunks of 8 blocks (the int32-intermediate kernels)."""
+        four bytes in two K chunks of 8 blocks (the int32-intermediate kernels).
+        fold: stage A without its bias correction, stage B initialised with
+        the constant that cancels it (the batch kernels)."""
         x = np.asarray(x, dtype=np.int16).reshape(-1, 256)
         P = x.shape[0]
         u = x.view(np.uint16).astype(np.int64) ^ 0x8000                   # x + 32768
@@ -144,7 +155,7 @@ class InvModel:
                 v = u[:, [16 * b + 2 * fwd_slot_e(j) + s for j in range(8)]]
                 B = np.stack([v & 255, v >> 8], axis=2).reshape(P, 16)
                 D = B @ self.AA[b][s].T
-                S = D[:, :8] + self.corr[b, s][None, :] + 128 * D[:, 8:]
+                S = D[:, :8] + (0 if fold else self.corr[b, s][None, :]) + 128 * D[:, 8:]
                 assert S.min() >= 0 and S.max() < (1 << (24 if wide else 25))
                 r = S if wide else S - ((S * BAR_LAZY) >> 32) * Q
                 for a in range(8):
@@ -162,7 +173,7 @@ class InvModel:
             X = np.stack([m & 255, m >> 8], axis=2).reshape(P, 32, 16)
             D0 = np.einsum("ik,pkc->pic", self.AB[0], X)
             D1 = np.einsum("ik,pkc->pic", self.AB[1], X)
-        S = D0 + 128 * D1
+        S = D0 + 128 * D1 + (self.binit[None, :, :] if fold else 0)
         # centred reduction: floor((S + 1664) / q) from the exact multiplier
         assert S.min() >= 0 and S.max() + 1664 < (1 << 26)
         r = S - (((S + 1664) * BAR_EXACT) >> 38) * Q

@@ -61,6 +61,9 @@ def test_kernel_arithmetic_model(tk, oracle, lo, hi, wide):
     f = fw(x, wide=wide)
     assert f.min() >= 0 and f.max() < Q
     assert (f == canon(oracle.ntt(ref_in))).all()
+    v = iv(x, wide=wide, fold=True)
+    assert v.min() >= -(Q // 2) and v.max() <= Q // 2
+    assert (canon(v) == canon(oracle.invntt(ref_in))).all()
     v = iv(x, wide=wide)
     assert v.min() >= -(Q // 2) and v.max() <= Q // 2
     assert (canon(v) == canon(oracle.invntt(ref_in))).all()
@@ -75,6 +78,7 @@ def test_kernel_model_extreme_rows(tk, oracle, wide):
     ref_in = canon(x).astype(np.int16)
     assert (fw(x, wide=wide) == canon(oracle.ntt(ref_in))).all()
     assert (canon(iv(x, wide=wide)) == canon(oracle.invntt(ref_in))).all()
+    assert (canon(iv(x, wide=wide, fold=True)) == canon(oracle.invntt(ref_in))).all()
 
 
 @pytest.mark.parametrize("lo,hi", [(-128, 128), (-3, 4), (-1, 2)])
