@@ -55,7 +55,8 @@ def parse():
                    help="fused ML-KEM matrix-vector jobs, k ~ U{2,3,4} (eager and CUDA graph)")
     p.add_argument("--jobs", type=int, default=65536)
     p.add_argument("--chunk", type=int, default=0, help="tk_matvec chunk (vector polys), 0 = default")
-    p.add_argument("--matvec-mode", type=int, default=0, help="0 pipeline, 1 fused single launch")
+    p.add_argument("--matvec-mode", type=int, default=2,
+                   help="0 pipeline, 1 fused single launch, 2 tiled (the default)")
     p.add_argument("--forms", action="store_true",
                    help="forward NTT by input form (int16, small, packed 2/3-bit)")
     p.add_argument("--serve", action="store_true",
@@ -539,7 +540,7 @@ def run_matvec(args):
         "jobs_per_k": {str(k): int((ks == k).sum()) for k in (2, 3, 4)},
         "config": {"workload": f"{args.jobs} jobs, A k x k uniform [0,q) NTT domain, s,e in [-3,3]",
                    "chunk_vec_polys": tk.get_option(tk.OPT_MATVEC_CHUNK_POLYS),
-                   "mode": ["pipeline", "fused"][tk.get_option(tk.OPT_MATVEC_MODE)]},
+                   "mode": ["pipeline", "fused", "tiled"][tk.get_option(tk.OPT_MATVEC_MODE)]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "bytes_per_step": nbytes,
                      "peak_source": peak_kind},

@@ -195,8 +195,10 @@ int tk_server_destroy(tk_server *srv, double timeout_s);
  * TK_OPT_MATVEC_CHUNK_POLYS: vector polynomials per tk_matvec chunk (the
  * chunk's intermediates are meant to stay in L2); 0 restores the default.
  * TK_OPT_MATVEC_MODE: TK_MATVEC_PIPELINE (NTT, basemul-accumulate and iNTT+e
- * as three stream-ordered kernels per chunk) or TK_MATVEC_FUSED (one kernel,
- * one warp per job: every intermediate stays in shared memory).
+ * as three stream-ordered kernels per chunk), TK_MATVEC_FUSED (one kernel,
+ * one warp per job: every intermediate stays in shared memory) or
+ * TK_MATVEC_TILED (the default: one kernel for up to four batches, a CTA
+ * carries a tile of 8 or 16 jobs through all three steps in shared memory).
  * TK_OPT_HOST_CHUNK_POLYS: largest number of polynomials per copy-in /
  * transform / copy-out chunk of tk_ntt_host / tk_invntt_host (1 .. 32768, the
  * default; smaller chunks are slower on a B200 host link: the path runs at the
@@ -207,6 +209,7 @@ int tk_server_destroy(tk_server *srv, double timeout_s);
 #define TK_OPT_HOST_CHUNK_POLYS 3
 #define TK_MATVEC_PIPELINE 0
 #define TK_MATVEC_FUSED 1
+#define TK_MATVEC_TILED 2
 int tk_set_option(int option, long long value);
 long long tk_get_option(int option);
 
@@ -220,12 +223,14 @@ int tk_init(int device);
 
 /* Reads and clears the kernel-side error flags of a device (bit 0: forward,
  * bit 1: inverse kernel gave up on a bounded wait; bit 2: tk_ntt_small saw a
- * coefficient outside [-128, 127]; bit 3: tk_selftest_bounded_wait).
+ * coefficient outside [-128, 127]; bit 3: tk_selftest_bounded_wait; bit 4:
+ * the TK_MATVEC_TILED kernel gave up on a bounded wait).
  * Synchronous. */
 #define TK_FLAG_FORWARD_TIMEOUT 1u
 #define TK_FLAG_INVERSE_TIMEOUT 2u
 #define TK_FLAG_SMALL_RANGE 4u
 #define TK_FLAG_SELFTEST_TIMEOUT 8u
+#define TK_FLAG_MATVEC_TIMEOUT 16u
 int tk_device_status(int device, unsigned *flags);
 /* Exercises the kernels' give-up path: one CTA waits on an mbarrier that
  * nothing completes, through the same bounded wait as the batch kernels, and

@@ -245,6 +245,7 @@ def invntt_host(a: np.ndarray) -> np.ndarray:
 
 
 FLAG_FORWARD_TIMEOUT, FLAG_INVERSE_TIMEOUT, FLAG_SMALL_RANGE, FLAG_SELFTEST_TIMEOUT = 1, 2, 4, 8
+FLAG_MATVEC_TIMEOUT = 16
 
 
 def ntt_small(polys, out=None, stream=None):
@@ -405,7 +406,7 @@ class Server:
 OPT_MATVEC_CHUNK_POLYS = 1
 OPT_HOST_CHUNK_POLYS = 3
 OPT_MATVEC_MODE = 2
-MATVEC_PIPELINE, MATVEC_FUSED = 0, 1
+MATVEC_PIPELINE, MATVEC_FUSED, MATVEC_TILED = 0, 1, 2
 
 
 def set_option(option: int, value: int) -> None:

@@ -48,7 +48,7 @@ std::atomic<long long> g_matvec_chunk{tk::kMatvecChunkVecPolys};
 constexpr size_t kHostStagePolys = (size_t)1 << 15;  // 16 MiB per staging buffer
 constexpr long long kHostChunkDefault = 1 << 15;
 std::atomic<long long> g_host_chunk{kHostChunkDefault};
-std::atomic<int> g_matvec_mode{TK_MATVEC_PIPELINE};
+std::atomic<int> g_matvec_mode{TK_MATVEC_TILED};
 
 const char* const kVariantNames[tk::kNumMmaVariants] = {
     "mma.sync 4 warps x 32-poly tiles, 3-slot TMA ring",
@@ -480,7 +480,27 @@ static int validate_matvec(const tk_matvec_batch* batches, int nbatches, bool ho
 // Launches a validated batch list of device buffers.
 static int launch_matvec_batches(const tk_matvec_batch* batches, int nbatches,
                                  const DeviceInfo* info, cudaStream_t stream) {
-  if (g_matvec_mode.load(std::memory_order_relaxed) == TK_MATVEC_FUSED) {
+  const int mode = g_matvec_mode.load(std::memory_order_relaxed);
+  if (mode == TK_MATVEC_TILED) {  // one tile-kernel launch per kMaxSegs batches
+    tk::MatvecPart parts[tk::kMaxSegs];
+    int np = 0;
+    for (int b = 0; b <= nbatches; b++) {
+      if (b < nbatches && batches[b].njobs != 0) {
+        const tk_matvec_batch& B = batches[b];
+        parts[np++] = tk::MatvecPart{B.k, B.njobs, B.A, B.s, B.e, B.out};
+      }
+      if (np == tk::kMaxSegs || (b == nbatches && np > 0)) {
+        cudaError_t e = tk::launch_matvec_tile(parts, np, *info, stream);
+        if (e != cudaSuccess) {
+          set_launch_err(e);
+          return TK_ERR_CUDA;
+        }
+        np = 0;
+      }
+    }
+    return TK_SUCCESS;
+  }
+  if (mode == TK_MATVEC_FUSED) {
     // single-launch fused kernel, up to three batches per launch
     tk::FusedBatches fb{};
     int b = 0;
@@ -848,7 +868,8 @@ int tk_set_option(int option, long long value) {
       g_matvec_chunk.store(value == 0 ? tk::kMatvecChunkVecPolys : value);
       return TK_SUCCESS;
     case TK_OPT_MATVEC_MODE:
-      if (value != TK_MATVEC_PIPELINE && value != TK_MATVEC_FUSED) break;
+      if (value != TK_MATVEC_PIPELINE && value != TK_MATVEC_FUSED && value != TK_MATVEC_TILED)
+        break;
       g_matvec_mode.store((int)value);
       return TK_SUCCESS;
     case TK_OPT_HOST_CHUNK_POLYS:

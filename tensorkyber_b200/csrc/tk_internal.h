@@ -28,6 +28,7 @@ struct DeviceInfo {
   int form_ctas_per_sm[kNumInputForms] = {1, 1, 1};  // forward input forms 1..3
   int add_ctas_per_sm[kNumMmaVariants] = {1, 1, 1, 1};  // inverse with addend
   int multi_ctas_per_sm[3] = {1, 1, 1};  // multi-segment forward / inverse / inverse+addend
+  int tile_ctas_per_sm = 1;              // k_matvec_tiles
   size_t total_mem = 0;
 };
 
@@ -98,6 +99,11 @@ struct MatvecPart {
 cudaError_t launch_matvec(const MatvecPart* batches, int nb, const DeviceInfo& info,
                           cudaStream_t stream, int fwd_variant, int inv_variant,
                           long long chunk_vec_polys);
+// The tiled single-kernel form: one k_matvec_tiles launch for up to kMaxSegs
+// batches (forward NTT, basemul-accumulate and inverse NTT + e of a tile of
+// jobs in one CTA's shared memory).
+cudaError_t launch_matvec_tile(const MatvecPart* batches, int nb, const DeviceInfo& info,
+                               cudaStream_t stream);
 
 // ---- serving loop (device side in tk_matvec.cu, host side in tk_serve.cpp) ----
 // One job descriptor of the job ring (64 bytes; the ring lives in mapped

@@ -31,34 +31,20 @@
 
 namespace tk {
 
-// Pair constants: pair t (coefficients 2t, 2t+1) of the NTT domain is the
-// residue mod X^2 - z_t, z_t = +-17^brv7(64 + t/2) (sign + for even t); the
-// reference's basemul multiplies by 2^-16 (Montgomery).  g_bm_zr[t] =
-// z_t * 2^-16 mod q.
+// Pair constants z_t * 2^-16 mod q (build_pair_constants).
 __device__ int32_t g_bm_zr[128];
 
-constexpr uint32_t kRinv = 169;               // 2^-16 mod q
 constexpr uint32_t kAccBias = 1073742318u;    // q * ceil(2^30 / q)
 
 __device__ __forceinline__ uint32_t mulmod_lazy(uint32_t x, uint32_t c) {
   return red_lazy(x * c);  // x < q + 8, c < q: x * c < 2^24
 }
-// S in [0, 2^31): representative in [0, 3q).
-__device__ __forceinline__ uint32_t red_wide(uint32_t s) {
-  return s - __umulhi(s, 1290167u) * 3329u;
-}
 
 // One warp per job; lane l owns coefficient pairs 4l .. 4l+3 (16 bytes of every
 // polynomial).  vec holds ntt(s) on entry and the accumulated products on
 // exit.  All k + k^2 loads of a job are issued before any arithmetic (the
-// kernel streams A from HBM and is bound by loads in flight), and the raw
-// products are accumulated first: per pair t with z = z_t,
-//   out0 = 2^-16 (sum_j a0 b0 + z sum_j a1 b1),  out1 = 2^-16 sum_j (a0 b1 + a1 b0)
-// so the constants (2^-16 and z 2^-16, g_bm_zr) are applied once per output
-// pair rather than to every ntt(s) coefficient.  |sum| < 2k * 32768 * q < 2^30
-// for k <= 4.
-constexpr uint32_t kSumBias = 3329u * 262144u;  // > 2^29.7 >= |sum|; sum + bias < 2^31
-
+// kernel streams A from HBM and is bound by loads in flight); the products
+// are accumulated as in basemul_row.
 template <int K>
 __global__ void __launch_bounds__(256) k_basemul_acc(const int16_t* __restrict__ A,
                                                      int16_t* __restrict__ vec, int njobs) {
@@ -81,43 +67,14 @@ __global__ void __launch_bounds__(256) k_basemul_acc(const int16_t* __restrict__
       for (int j = 0; j < K; j++)
         a[i][j] = __ldcs((const uint4*)(A + (((size_t)job * K + i) * K + j) * 256 + 8 * lane));
 #pragma unroll
-    for (int i = 0; i < K; i++) {
-      uint32_t o[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        int32_t t00 = 0, t11 = 0, t1 = 0;
-#pragma unroll
-        for (int j = 0; j < K; j++) {
-          const uint32_t aw = u == 0 ? a[i][j].x : u == 1 ? a[i][j].y : u == 2 ? a[i][j].z : a[i][j].w;
-          const uint32_t bw = u == 0 ? b[j].x : u == 1 ? b[j].y : u == 2 ? b[j].z : b[j].w;
-          const int32_t a0 = (int16_t)(aw & 0xffffu), a1 = (int32_t)aw >> 16;
-          const int32_t b0 = (int32_t)(bw & 0xffffu), b1 = (int32_t)(bw >> 16);  // [0, q)
-          t00 += a0 * b0;
-          t11 += a1 * b1;
-          t1 += a0 * b1 + a1 * b0;
-        }
-        const uint32_t r00 = red_wide((uint32_t)t00 + kSumBias);  // [0, 3q)
-        const uint32_t r11 = red_wide((uint32_t)t11 + kSumBias);
-        const uint32_t r1 = red_wide((uint32_t)t1 + kSumBias);
-        // r00 * 169 + r11 * zr < 3q * 169 + 3q * q < 2^31
-        o[u] = pack2(red_wide(r00 * kRinv + r11 * zr[u]), red_wide(r1 * kRinv));
-      }
-      *(uint4*)(vec + ((size_t)job * K + i) * 256 + 8 * lane) = make_uint4(o[0], o[1], o[2], o[3]);
-    }
+    for (int i = 0; i < K; i++)
+      *(uint4*)(vec + ((size_t)job * K + i) * 256 + 8 * lane) = basemul_row<K>(a[i], b, zr);
   }
 }
 
 static bool upload_pair_constants() {
-  // z_t = +-17^brv7(64 + t/2) mod q, times 2^-16
   int32_t zr[128];
-  for (int t = 0; t < 128; t++) {
-    unsigned k = 64 + t / 2, r = 0;
-    for (int b = 0; b < 7; b++) r |= ((k >> b) & 1u) << (6 - b);
-    int64_t z = 1;
-    for (unsigned e = 0; e < r; e++) z = z * 17 % 3329;
-    if (t & 1) z = (3329 - z) % 3329;
-    zr[t] = (int32_t)(z * kRinv % 3329);
-  }
+  build_pair_constants(zr);
   return cudaMemcpyToSymbol(g_bm_zr, zr, sizeof(zr)) == cudaSuccess;
 }
 

@@ -122,24 +122,24 @@ __device__ __forceinline__ void cta_sync_named() {
   asm volatile("bar.sync 1;" ::: "memory");
 }
 
-// Block-wise stage of one tile for this warp: P block pairs x W n-tiles of 8
-// polynomials, the next unit's ldmatrix issued ahead of the current stores.
-// Inverse input is biased (x ^ 0x8000) and parity-split here; forward input
-// is already parity-split by stage 1.
-template <bool kInverse, int W, int P>
+// Block-wise stage of one tile for this warp: P block pairs x NT n-tiles of 8
+// polynomials (NT = W: a full tile), the next unit's ldmatrix issued ahead of
+// the current stores.  Inverse input is biased (x ^ 0x8000) and parity-split
+// here; forward input is already parity-split by stage 1.
+template <bool kInverse, int W, int P, int NT = W>
 __device__ __forceinline__ void block_stage(uint32_t slot, uint8_t* slotp, int blk0,
                                             uint32_t ldc_off, uint32_t stc_off,
                                             const uint32_t (&ac)[P][2][2][2],
                                             const int32_t (&cc)[P][2][2]) {
-  constexpr int kIters = P * W;
+  constexpr int kIters = P * NT;
   uint32_t r[4];
   ldsm_x4(slot + 32u * blk0 + ldc_off, r[0], r[1], r[2], r[3]);
 #pragma unroll
   for (int it = 0; it < kIters; it++) {
-    const int p = it / W, nt = it % W;
+    const int p = it / NT, nt = it % NT;
     uint32_t n[4] = {0, 0, 0, 0};
     if (it + 1 < kIters) {
-      const int p1 = (it + 1) / W, nt1 = (it + 1) % W;
+      const int p1 = (it + 1) / NT, nt1 = (it + 1) % NT;
       ldsm_x4(slot + nt1 * 8 * kRowBytes + 32u * (blk0 + 2 * p1) + ldc_off, n[0], n[1], n[2],
               n[3]);
     }
@@ -673,6 +673,247 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn, kWide>::kMinBlocks)
   if (kIn == kInSmall && __any_sync(0xffffffffu, bad != 0) && lane == 0) atomicOr(&g_status, 4u);
 }
 
+// -------------------------------------------------- matrix-vector tiles ---
+// k_matvec_tiles: ML-KEM matrix-vector jobs of up to kMaxSegs batches (one k
+// each) in one launch,
+//     out_i = invntt( sum_j basemul(A_ij, ntt(s_j)) ) + e_i,
+// with all three steps on one CTA's shared memory.  A tile is kJobs(k)
+// consecutive jobs of one batch, i.e. kRows(k) = kJobs * k consecutive vector
+// rows of its s / e / out (32 for k = 2, 4; 24 for k = 3): 8-row TMA boxes in,
+// the forward NTT in place (the batch kernels' stages: by polynomial, CTA
+// barrier, by block over the tile's n-tiles), the basemul-accumulate by job
+// (warp w: jobs w, w+4, ...; ntt(s) from shared memory, all k^2 loads of A from
+// global memory issued first, A and e prefetched into L2 one tile ahead with
+// bulk prefetches), the inverse NTT plus e in place on the accumulator tile (e
+// read in stage B, as the batch inverse with addend), 8-row TMA boxes out.
+// Tiles are numbered across the batches (batch b owns [first_tile[b],
+// first_tile[b+1])) and CTA c takes tiles c, c + G, c + 2G, ... (G CTAs), so
+// the launch has one tail for all batches and its CTAs run one k at a time.  s tiles are double-buffered (the next
+// tile's load runs under this tile's work); the accumulator tile is reused
+// once its previous store has been read out.  Rows past a batch are out of
+// bounds of its tensor maps (zero-filled in; boxes that start past it are
+// neither loaded nor stored) and jobs past it are skipped.  The stage
+// constants are re-read from L1 at each stage, so that between stages their
+// registers hold the basemul's loads in flight.  Every mbarrier wait is
+// bounded (2 s; sets status bit 4 and stops the CTA).
+struct MvTiles {
+  CUtensorMap s_map[kMaxSegs];    // s rows [njobs * k][128 words], 8 x 132-word boxes
+  CUtensorMap out_map[kMaxSegs];  // out rows, the same shape (may equal s_map: in place)
+  const int16_t* A[kMaxSegs];     // [njobs][k][k][256]
+  const uint32_t* e[kMaxSegs];    // [njobs][k][256] as words, or null
+  int njobs[kMaxSegs];
+  int k[kMaxSegs];
+  int first_tile[kMaxSegs + 1];
+  int nb;
+};
+
+__device__ int32_t g_tile_zr[128];  // basemul pair constants (build_pair_constants)
+
+constexpr int kTileSlotBytes = 32 * kRowBytes;      // one 32-row slot
+constexpr int kTileSmem = 3 * kTileSlotBytes + 16;  // s slot x 2, accumulators, 2 mbarriers
+__host__ __device__ constexpr int tile_units(int k) { return k == 3 ? 3 : 4; }
+__host__ __device__ constexpr int tile_jobs(int k) { return 8 * tile_units(k) / k; }
+
+__global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__ MvTiles P) {
+  constexpr int W = 4, PP = 2;  // PP: block pairs per warp
+  extern __shared__ __align__(128) uint8_t smem[];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int ntiles = P.first_tile[P.nb];
+  // tiles c, c + G, c + 2G, ...: all CTAs move through the batches together
+  // (one k's code at a time)
+  const int G = (int)gridDim.x;
+  const int nmine = ntiles > (int)blockIdx.x ? (ntiles - 1 - (int)blockIdx.x) / G + 1 : 0;
+  const uint32_t smem0 = smem_u32(smem);
+  const uint32_t acc = smem0 + 2 * kTileSlotBytes;
+  uint8_t* const accp = smem + 2 * kTileSlotBytes;
+  const uint32_t bar0 = smem0 + 3 * kTileSlotBytes;
+
+  const int blk0 = 4 * warp;
+  int32_t zc[PP][2][2];
+#pragma unroll
+  for (int p = 0; p < PP; p++)
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int s = 0; s < 2; s++) zc[p][h][s] = 0;
+  auto load_am = [&](const uint32_t (*src)[32][4], uint32_t (&am)[2][4]) {
+#pragma unroll
+    for (int g = 0; g < 2; g++) {
+      const uint4 v = ldg_keep_u4(&src[g][lane][0]);
+      am[g][0] = v.x;
+      am[g][1] = v.y;
+      am[g][2] = v.z;
+      am[g][3] = v.w;
+    }
+  };
+  auto load_ac = [&](const uint32_t (*src)[2][32][2], uint32_t (&ac)[PP][2][2][2]) {
+#pragma unroll
+    for (int p = 0; p < PP; p++)
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+          const uint2 v = ldg_keep_u2(&src[blk0 + 2 * p + h][s][lane][0]);
+          ac[p][h][s][0] = v.x;
+          ac[p][h][s][1] = v.y;
+        }
+  };
+  uint32_t zr[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) zr[u] = (uint32_t)g_tile_zr[4 * lane + u];
+
+  if (tid == 0) {
+    mbar_init(bar0, W);
+    mbar_init(bar0 + 8, W);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  grid_dependency_wait();
+  grid_launch_dependents();
+  if (nmine <= 0) return;
+
+  const int q4 = lane & 3, g8 = lane >> 2;
+  const uint32_t ldt_off = 32u * ((lane & 7) + 8 * ((lane >> 3) & 1)) + 16u * (lane >> 4);
+  const uint32_t hb1 = (lane >> 4) & 1;
+  const uint32_t w_even = 32u * g8 + 16u * hb1 + 4u * q4;
+  const uint32_t w_odd = 32u * g8 + 16u * (hb1 ^ 1) + 4u * q4;
+  const uint32_t w_nat = 32u * g8 + 4u * q4;
+  const uint32_t hbw = (uint32_t)((blk0 >> 2) & 1);
+  const uint32_t ldc_base = kRowBytes * (lane & 7) + 32u * (lane >> 4);
+  const uint32_t ldc_fwd = ldc_base + 16u * (((lane >> 3) & 1) ^ hbw);
+  const uint32_t ldc_inv = ldc_base + 16u * ((lane >> 3) & 1);
+  const uint32_t stc_off = kRowBytes * (2 * q4) + 4u * g8;
+
+  auto batch_of = [&](int t) {
+    int b = 0;
+#pragma unroll
+    for (int j = 1; j < kMaxSegs; j++) b += (j < P.nb && t >= P.first_tile[j]);
+    return b;
+  };
+  auto issue_load = [&](int k, int slot_i) {
+    if (lane != 0) return;
+    const uint32_t bar = bar0 + 8 * slot_i;
+    const int t = (int)blockIdx.x + k * G, b = batch_of(t), kb = P.k[b];
+    const int row = (t - P.first_tile[b]) * 8 * tile_units(kb) + 8 * warp;
+    if (warp < tile_units(kb) && row < P.njobs[b] * kb) {  // boxes past the batch: none
+      mbar_expect_tx(bar, kWarpBoxBytes);
+      tma_load_2d(smem0 + slot_i * kTileSlotBytes + warp * kWarpBoxBytes, &P.s_map[b], 0, row,
+                  bar);
+    } else {
+      mbar_expect_tx(bar, 0);  // arrive only
+    }
+  };
+  // A and e of tile k into L2 (one thread; the ranges stop at the batch end)
+  auto prefetch = [&](int k) {
+    if (tid != 0) return;
+    const int t = (int)blockIdx.x + k * G, b = batch_of(t), kb = P.k[b];
+    const int j0 = (t - P.first_tile[b]) * tile_jobs(kb);
+    const int nj = min(tile_jobs(kb), P.njobs[b] - j0);
+    bulk_prefetch_l2(P.A[b] + (size_t)j0 * kb * kb * 256, (uint32_t)nj * kb * kb * 512u);
+    if (P.e[b]) bulk_prefetch_l2(P.e[b] + (size_t)j0 * kb * 128, (uint32_t)nj * kb * 512u);
+  };
+
+  // one tile of batch b (k = K), its s in the given slot
+  auto run_tile = [&](auto kc, int b, int tl, uint32_t slot, uint8_t* slotp) {
+    constexpr int K = decltype(kc)::value;
+    constexpr int NU = tile_units(K), kJobs = tile_jobs(K);
+    const int njobs = P.njobs[b], nvec = njobs * K, row0 = tl * 8 * NU;
+
+    // forward NTT of the s tile, in place
+    if (warp < NU) {
+      uint32_t fam[2][4];
+      load_am(g_fwd.s1, fam);
+      const uint2 c1 = ldg_keep_u2(&g_fwd.c1[lane][0]);
+      const int32_t cbz[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+      poly_stage<false>(slot + 8 * warp * kRowBytes, slotp + 8 * warp * kRowBytes, ldt_off, fam,
+                        (int32_t)c1.x, (int32_t)c1.y, cbz, w_even, w_odd, 0, nullptr, 0, 0, 0);
+    }
+    cta_sync_named();
+    {
+      uint32_t fac[PP][2][2][2];
+      load_ac(g_fwd.s2, fac);
+      block_stage<false, W, PP, NU>(slot, slotp, blk0, ldc_fwd, stc_off, fac, zc);
+    }
+    if (lane == 0) bulk_wait_read<0>();  // the accumulators' last store has been read out
+    cta_sync_named();
+
+    // basemul-accumulate into the accumulator tile, one job per warp at a
+    // time, all k^2 loads of A issued first
+    for (int jl = warp; jl < kJobs; jl += W) {
+      const int job = tl * kJobs + jl;
+      if (job >= njobs) break;  // warp-uniform
+      const int16_t* Aj = P.A[b] + (size_t)job * K * K * 256 + 8 * lane;
+      uint4 a[K][K], bv[K];
+#pragma unroll
+      for (int i = 0; i < K; i++)
+#pragma unroll
+        for (int j = 0; j < K; j++) a[i][j] = __ldcs((const uint4*)(Aj + (i * K + j) * 256));
+#pragma unroll
+      for (int j = 0; j < K; j++)
+        bv[j] = *(const uint4*)(slotp + (jl * K + j) * kRowBytes + 16 * lane);
+#pragma unroll
+      for (int i = 0; i < K; i++)
+        *(uint4*)(accp + (jl * K + i) * kRowBytes + 16 * lane) = basemul_row<K>(a[i], bv, zr);
+    }
+    cta_sync_named();
+
+    // inverse NTT plus e on the accumulator tile, in place; then the store
+    {
+      uint32_t iac[PP][2][2][2];
+      load_ac(g_inv.sa, iac);
+      block_stage<true, W, PP, NU>(acc, accp, blk0, ldc_inv, stc_off, iac, zc);
+    }
+    cta_sync_named();
+    if (warp < NU) {
+      uint32_t iam[2][4];
+      load_am(g_inv.sb, iam);
+      int32_t cb[2][4];
+#pragma unroll
+      for (int t = 0; t < 2; t++) {
+        const uint4 v = ldg_keep_u4(&g_inv.cbz[lane][t][0]);
+        cb[t][0] = (int32_t)v.x;
+        cb[t][1] = (int32_t)v.y;
+        cb[t][2] = (int32_t)v.z;
+        cb[t][3] = (int32_t)v.w;
+      }
+      poly_stage<true, true>(acc + 8 * warp * kRowBytes, accp + 8 * warp * kRowBytes, ldt_off, iam,
+                             0, 0, cb, 0, 0, w_nat, P.e[b], row0 + 8 * warp, nvec, 8u * g8 + q4);
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0 && row0 + 8 * warp < nvec)  // boxes past the batch are dropped
+        tma_store_2d(&P.out_map[b], 0, row0 + 8 * warp, acc + warp * kWarpBoxBytes);
+    }
+    if (lane == 0) bulk_commit();  // every lane-0 keeps one (possibly empty) group per tile
+  };
+
+  issue_load(0, 0);
+  prefetch(0);
+  for (int k = 0; k < nmine; k++) {
+    const int slot_i = k & 1;
+    const uint32_t slot = smem0 + slot_i * kTileSlotBytes;
+    uint8_t* const slotp = smem + slot_i * kTileSlotBytes;
+    const bool ok = mbar_wait_bounded(bar0 + 8 * slot_i, (uint32_t)(k >> 1) & 1u, kWaitLimitNs);
+    if (!__syncthreads_and(ok)) {  // CTA-uniform give-up
+      if (tid == 0) atomicOr(&g_status, 16u);
+      break;
+    }
+    // the other slot held tile k-1's s, finished before the barrier above
+    if (k + 1 < nmine) {
+      issue_load(k + 1, slot_i ^ 1);
+      prefetch(k + 1);
+    }
+    const int t = (int)blockIdx.x + k * G, b = batch_of(t), tl = t - P.first_tile[b];
+    switch (P.k[b]) {  // CTA-uniform
+      case 2: run_tile(std::integral_constant<int, 2>{}, b, tl, slot, slotp); break;
+      case 3: run_tile(std::integral_constant<int, 3>{}, b, tl, slot, slotp); break;
+      default: run_tile(std::integral_constant<int, 4>{}, b, tl, slot, slotp); break;
+    }
+  }
+  if (lane == 0) bulk_wait_all();
+}
+
 // ------------------------------------------------------------ host side ----
 struct Variant {
   const void* fn;
@@ -786,6 +1027,9 @@ static bool upload_tables_current_device() {
   });
   if (cudaMemcpyToSymbol(g_fwd, &FF, sizeof(FF)) != cudaSuccess) return false;
   if (cudaMemcpyToSymbol(g_inv, &IF, sizeof(IF)) != cudaSuccess) return false;
+  int32_t zr[128];
+  build_pair_constants(zr);
+  if (cudaMemcpyToSymbol(g_tile_zr, zr, sizeof(zr)) != cudaSuccess) return false;
   const unsigned zero = 0;
   return cudaMemcpyToSymbol(g_status, &zero, sizeof(zero)) == cudaSuccess;
 }
@@ -825,6 +1069,16 @@ bool mma_init_device(DeviceInfo* info) {
         cudaSuccess)
       return false;
     info->multi_ctas_per_sm[m] = per_sm > 0 ? per_sm : 1;
+  }
+  {
+    const void* fn = (const void*)k_matvec_tiles;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem) !=
+        cudaSuccess)
+      return false;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, kTileSmem) != cudaSuccess)
+      return false;
+    info->tile_ctas_per_sm = per_sm > 0 ? per_sm : 1;
   }
   for (int f = 0; f < kNumInputForms; f++) {
     const Variant& V = kFormVariants[f];
@@ -959,6 +1213,46 @@ cudaError_t launch_mma(bool inverse, int variant, const int16_t* src, int16_t* d
                        const int16_t* addend) {
   const Seg g{src, dst, npoly, addend};
   return launch_mma_segs(inverse, variant, &g, 1, info, stream);
+}
+
+cudaError_t launch_matvec_tile(const MatvecPart* batches, int nb, const DeviceInfo& info,
+                               cudaStream_t stream) {
+  if (nb > kMaxSegs) return cudaErrorInvalidValue;
+  MvTiles m = {};
+  for (int b = 0; b < nb; b++) {
+    const MatvecPart& B = batches[b];
+    // rows are 32-bit TMA coordinates and tile numbers 32-bit integers
+    if (B.njobs * (size_t)B.k > (size_t)kMaxLaunchPolys) return cudaErrorInvalidValue;
+    const int nvec = (int)(B.njobs * B.k);
+    if (!encode_batch_map(&m.s_map[b], B.s, nvec)) return cudaErrorInvalidResourceHandle;
+    if (B.out == B.s)
+      m.out_map[b] = m.s_map[b];
+    else if (!encode_batch_map(&m.out_map[b], B.out, nvec))
+      return cudaErrorInvalidResourceHandle;
+    m.A[b] = B.A;
+    m.e[b] = (const uint32_t*)B.e;
+    m.njobs[b] = (int)B.njobs;
+    m.k[b] = B.k;
+    const int tj = tile_jobs(B.k);
+    m.first_tile[b + 1] = m.first_tile[b] + (int)((B.njobs + tj - 1) / tj);
+  }
+  m.nb = nb;
+  long long ctas = m.first_tile[nb];
+  if (ctas <= 0) return cudaSuccess;
+  const long long cap = (long long)info.num_sms * info.tile_ctas_per_sm;
+  if (ctas > cap) ctas = cap;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)ctas);
+  cfg.blockDim = dim3(128);
+  cfg.dynamicSmemBytes = (size_t)kTileSmem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* args[1] = {(void*)&m};
+  return cudaLaunchKernelExC(&cfg, (const void*)k_matvec_tiles, args);
 }
 
 // Self-test of the give-up path: one CTA waits, through the same bounded

@@ -280,4 +280,47 @@ __device__ __forceinline__ void stage_c_inv_wide(const uint32_t (&a)[2][2][2],
       *(uint2*)(rows + j * kWideRowBytes + off[s]) = make_uint2(S[s][j][0], S[s][j][1]);
 }
 
+// ------------------------------------------------------------- basemul ----
+constexpr uint32_t kRinv = 169;                 // 2^-16 mod q
+constexpr uint32_t kSumBias = 3329u * 262144u;  // > 2^29.7 >= |sum|; sum + bias < 2^31
+
+// S in [0, 2^31): representative in [0, 3q).
+__device__ __forceinline__ uint32_t red_wide(uint32_t s) {
+  return s - __umulhi(s, 1290167u) * 3329u;
+}
+
+// One output polynomial of a job's basemul-accumulate for one lane, which
+// owns coefficient pairs 4l .. 4l+3 (16 bytes of every polynomial): a[j] =
+// those bytes of A_ij (any int16), b[j] = of ntt(s_j) (in [0, q)), zr = the
+// pairs' constants z_t * 2^-16.  The raw products are accumulated first, per
+// pair t with z = z_t:
+//   out0 = 2^-16 (sum_j a0 b0 + z sum_j a1 b1),  out1 = 2^-16 sum_j (a0 b1 + a1 b0)
+// so the constants are applied once per output pair.  |sum| < 2K * 32768 * q
+// < 2^30 for K <= 4.  Output pairs in [0, 3q).
+template <int K>
+__device__ __forceinline__ uint4 basemul_row(const uint4 (&a)[K], const uint4 (&b)[K],
+                                             const uint32_t (&zr)[4]) {
+  uint32_t o[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    int32_t t00 = 0, t11 = 0, t1 = 0;
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+      const uint32_t aw = u == 0 ? a[j].x : u == 1 ? a[j].y : u == 2 ? a[j].z : a[j].w;
+      const uint32_t bw = u == 0 ? b[j].x : u == 1 ? b[j].y : u == 2 ? b[j].z : b[j].w;
+      const int32_t a0 = (int16_t)(aw & 0xffffu), a1 = (int32_t)aw >> 16;
+      const int32_t b0 = (int32_t)(bw & 0xffffu), b1 = (int32_t)(bw >> 16);  // [0, q)
+      t00 += a0 * b0;
+      t11 += a1 * b1;
+      t1 += a0 * b1 + a1 * b0;
+    }
+    const uint32_t r00 = red_wide((uint32_t)t00 + kSumBias);  // [0, 3q)
+    const uint32_t r11 = red_wide((uint32_t)t11 + kSumBias);
+    const uint32_t r1 = red_wide((uint32_t)t1 + kSumBias);
+    // r00 * 169 + r11 * zr < 3q * 169 + 3q * q < 2^31
+    o[u] = pack2(red_wide(r00 * kRinv + r11 * zr[u]), red_wide(r1 * kRinv));
+  }
+  return make_uint4(o[0], o[1], o[2], o[3]);
+}
+
 }  // namespace tk

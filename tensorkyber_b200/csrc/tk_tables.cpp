@@ -82,6 +82,15 @@ int64_t byte_weighted(int64_t c, int byte) {
 
 }  // namespace
 
+void build_pair_constants(int32_t zr[128]) {
+  const int64_t rinv = 169;  // 2^-16 mod q
+  for (int t = 0; t < 128; t++) {
+    int64_t z = tw().w[64 + t / 2];
+    if (t & 1) z = modq(-z);
+    zr[t] = (int32_t)(z * rinv % kQ);
+  }
+}
+
 void build_matrices(Matrices* M) {
   int64_t v[256];
   for (int m = 0; m < 16; m++) {

@@ -111,6 +111,11 @@ struct Matrices {
   int16_t minv[16][16];      // [i][m]
 };
 
+// Basemul pair constants: pair t (coefficients 2t, 2t+1) of the NTT domain
+// is the residue mod X^2 - z_t, z_t = +-17^brv7(64 + t/2) (sign + for even t);
+// zr[t] = z_t * 2^-16 mod q (the reference's basemul multiplies by 2^-16).
+void build_pair_constants(int32_t zr[128]);
+
 void build_matrices(Matrices* M);
 void build_fwd_frags(const Matrices& M, FwdFrags* F);
 void build_inv_frags(const Matrices& M, InvFrags* F);

@@ -10,11 +10,12 @@ from py_oracle import Q, canon
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(params=[0, 1], ids=["pipeline", "fused"])
+@pytest.fixture(params=[0, 1, 2], ids=["pipeline", "fused", "tiled"])
 def mode(request, tk):
+    before = tk.get_option(tk.OPT_MATVEC_MODE)
     tk.set_option(tk.OPT_MATVEC_MODE, request.param)
     yield request.param
-    tk.set_option(tk.OPT_MATVEC_MODE, 0)
+    tk.set_option(tk.OPT_MATVEC_MODE, before)
 
 
 def make_jobs(seed, k, n, a_lo=0, a_hi=Q, small=3):
@@ -170,7 +171,8 @@ def test_matvec_pipeline_every_variant(tk, cuda, oracle, variant):
     """The pipeline's forward and inverse-with-addend launches in each batch
     kernel variant (one batch, so the single-batch kernels run)."""
     A, s, e = make_jobs(40 + variant, 3, 150)
-    tk.set_option(tk.OPT_MATVEC_MODE, 0)
+    before = tk.get_option(tk.OPT_MATVEC_MODE)
+    tk.set_option(tk.OPT_MATVEC_MODE, tk.MATVEC_PIPELINE)
     try:
         tk.set_variant(tk.FORWARD, variant)
         tk.set_variant(tk.INVERSE, variant)
@@ -178,4 +180,5 @@ def test_matvec_pipeline_every_variant(tk, cuda, oracle, variant):
     finally:
         tk.set_variant(tk.FORWARD, -1)
         tk.set_variant(tk.INVERSE, -1)
+        tk.set_option(tk.OPT_MATVEC_MODE, before)
     assert (canon(out) == canon(oracle_out(oracle, 3, A, s, e))).all()
