@@ -66,6 +66,8 @@ def parse():
                    help="offered load as multiples of the plain per-request capacity")
     p.add_argument("--serve-templates", type=int, default=256)
     p.add_argument("--serve-zero-copy", action="store_true")
+    p.add_argument("--serve-plain-mode", type=int, default=2,
+                   help="matrix-vector mode of the plain per-request path (0, 1, 2 as --matvec-mode)")
     return p.parse_args()
 
 
@@ -571,7 +573,7 @@ def run_serve(args):
 
     torch.cuda.set_device(0)
     tk.init(0)
-    tk.set_option(tk.OPT_MATVEC_MODE, tk.MATVEC_FUSED)
+    tk.set_option(tk.OPT_MATVEC_MODE, args.serve_plain_mode)
     L = tk.lib()
     r = np.random.default_rng(2025)
     T = args.serve_templates
@@ -706,7 +708,9 @@ def run_serve(args):
         "server_stats": stats, "clocks": clocks,
         "config": {"workload": "requests of 1-64 matrix-vector jobs, k ~ U{2,3,4}, "
                                "coefficients uniform [0,q), pinned host buffers (A|s|e contiguous)",
-                   "templates": T, "mode": "fused"},
+                   "templates": T,
+                   "plain_mode": ["pipeline", "fused", "tiled"][args.serve_plain_mode],
+                   "server": "fused warp-per-job device loop"},
         "dtype": "int16", "data": "synthetic",
     }), flush=True)
 
