@@ -320,12 +320,21 @@ __device__ __forceinline__ void poly_stage(uint32_t mine, uint8_t* minep, uint32
 // operands from the int16 rows (ldmatrix.trans as poly_stage, low bytes);
 // packed forms: from the tile's packed rows (packp: this warp's 8 rows of
 // kPackBytes), which lane (t = lane%4, n = lane/4) reads as the words of blocks
-// m = 2t, 2t+1, 8+2t, 9+2t.
-template <int kIn>
+// m = 2t, 2t+1, 8+2t, 9+2t.  Output to minep's rows (kRowBytes apart,
+// parity-split int16), or with kWideOut unreduced to int32 intermediate rows
+// (kWideRowBytes apart; w_even / w_odd then the wide offsets).
+template <int kIn, bool kWideOut = false>
 __device__ __forceinline__ void poly_stage_small(uint32_t mine, uint8_t* minep, uint32_t ldt_off,
                                                  const uint8_t* packp, const uint32_t (&ab)[2][2],
                                                  int32_t cb_lo, int32_t cb_hi, uint32_t w_even,
                                                  uint32_t w_odd, int lane, uint32_t* bad) {
+  constexpr int kOutRow = kWideOut ? kWideRowBytes : kRowBytes;
+  auto out = [&](int p, uint32_t bt0, uint32_t bt1) {
+    if constexpr (kWideOut)
+      stage_m_small_wide(ab, cb_lo, cb_hi, bt0, bt1, minep + p * kOutRow, w_even, w_odd);
+    else
+      stage_m_small(ab, cb_lo, cb_hi, bt0, bt1, minep + p * kOutRow, w_even, w_odd);
+  };
   const uint32_t t = lane & 3, n = lane >> 2;
   if (kIn == kInSmall) {
     uint32_t b[4];
@@ -336,7 +345,7 @@ __device__ __forceinline__ void poly_stage_small(uint32_t mine, uint8_t* minep, 
       if (p < 7) ldsm_x4_t(mine + (p + 1) * kRowBytes + ldt_off, nx[0], nx[1], nx[2], nx[3]);
       const uint32_t bt0 = small_operand(b[0], b[1], bad);
       const uint32_t bt1 = small_operand(b[2], b[3], bad);
-      stage_m_small(ab, cb_lo, cb_hi, bt0, bt1, minep + p * kRowBytes, w_even, w_odd);
+      out(p, bt0, bt1);
 #pragma unroll
       for (int j = 0; j < 4; j++) b[j] = nx[j];
     }
@@ -353,7 +362,7 @@ __device__ __forceinline__ void poly_stage_small(uint32_t mine, uint8_t* minep, 
       const uint2 v23 = *(const uint2*)(pk + 32 + 8 * t);  // m = 8+2t, 9+2t
       const uint32_t bt0 = packed_operand<2>(v01.x, v01.y, v23.x, v23.y, sel0, shift);
       const uint32_t bt1 = packed_operand<2>(v01.x, v01.y, v23.x, v23.y, sel1, shift);
-      stage_m_small(ab, cb_lo, cb_hi, bt0, bt1, minep + p * kRowBytes, w_even, w_odd);
+      out(p, bt0, bt1);
     }
   } else {
     // 8 bytes per block m; coefficient c is byte c/2, bits 3(c%2): n-tile 0
@@ -368,7 +377,7 @@ __device__ __forceinline__ void poly_stage_small(uint32_t mine, uint8_t* minep, 
       const uint4 v23 = *(const uint4*)(pk + 64 + 16 * t);  // m = 8+2t, 9+2t
       const uint32_t bt0 = packed_operand<3>(v01.x, v01.z, v23.x, v23.z, sel, shift);
       const uint32_t bt1 = packed_operand<3>(v01.y, v01.w, v23.y, v23.w, sel, shift);
-      stage_m_small(ab, cb_lo, cb_hi, bt0, bt1, minep + p * kRowBytes, w_even, w_odd);
+      out(p, bt0, bt1);
     }
   }
 }
@@ -381,8 +390,8 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn, kWide>::kMinBlocks)
   constexpr bool kMulti = std::is_same<Param, SegMaps>::value;
   static_assert(!kInverse || kIn == kInInt16, "input forms are forward only");
   static_assert(kInverse || !kAdd, "the addend is an inverse option");
-  static_assert(!kWide || (kIn == kInInt16 && !(kMulti && kInverse)),
-                "wide: int16 input; the inverse with one segment");
+  static_assert(!kWide || ((kIn == kInInt16 || !kInverse) && !(kMulti && kInverse)),
+                "wide: the inverse with int16 input and one segment");
   using C = Cfg<W, S, kIn, kWide>;
   extern __shared__ __align__(128) uint8_t smem[];
   const int tid = threadIdx.x;
@@ -616,17 +625,25 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn, kWide>::kMinBlocks)
       issue_store(k, slot_i);
     } else if constexpr (kWide) {
       uint8_t* irow0 = interp + 8 * warp * kWideRowBytes;
-      uint32_t b[4];
-      ldsm_x4_t(mine + ldt_off, b[0], b[1], b[2], b[3]);
+      if constexpr (kIn == kInInt16) {
+        uint32_t b[4];
+        ldsm_x4_t(mine + ldt_off, b[0], b[1], b[2], b[3]);
 #pragma unroll
-      for (int p = 0; p < 8; p++) {
-        uint32_t n[4] = {0, 0, 0, 0};
-        if (p < 7) ldsm_x4_t(mine + (p + 1) * kRowBytes + ldt_off, n[0], n[1], n[2], n[3]);
-        stage_m_wide(am, cm_lo, cm_hi, b[0] ^ 0x80008000u, b[1] ^ 0x80008000u,
-                     b[2] ^ 0x80008000u, b[3] ^ 0x80008000u, irow0 + p * kWideRowBytes, wi_e,
-                     wi_o);
+        for (int p = 0; p < 8; p++) {
+          uint32_t n[4] = {0, 0, 0, 0};
+          if (p < 7) ldsm_x4_t(mine + (p + 1) * kRowBytes + ldt_off, n[0], n[1], n[2], n[3]);
+          stage_m_wide(am, cm_lo, cm_hi, b[0] ^ 0x80008000u, b[1] ^ 0x80008000u,
+                       b[2] ^ 0x80008000u, b[3] ^ 0x80008000u, irow0 + p * kWideRowBytes, wi_e,
+                       wi_o);
 #pragma unroll
-        for (int j = 0; j < 4; j++) b[j] = n[j];
+          for (int j = 0; j < 4; j++) b[j] = n[j];
+        }
+      } else {
+        uint32_t tile_bad = 0;  // as below: only live rows count
+        poly_stage_small<kIn, true>(mine, irow0, ldt_off,
+                                    slotp + C::kRowsBytes + warp * 8 * C::kPackBytes, ab, cb_lo,
+                                    cb_hi, wi_e, wi_o, lane, &tile_bad);
+        if (u_begin + k * W + warp < u_end) bad |= tile_bad;
       }
       cta_sync_named();
       block_stage_wide<W>(inter, slotp, blk0, ldw, stc_off, ac);
@@ -951,12 +968,12 @@ static const Variant kMultiVariants[3] = {
     make_variant<true, 4, 3, kInInt16, false, SegMaps>(),
     make_variant<true, 4, 3, kInInt16, true, SegMaps>()};
 
-// Forward kernels for the small / packed input forms: 4 warps; 3 slots for
-// int16 rows, 2 for packed rows (their loads are 8x smaller, and the smaller
-// slots let 5 CTAs share an SM instead of 3).
-static const Variant kFormVariants[kNumInputForms] = {make_variant<false, 4, 3, kInSmall>(),
-                                                      make_variant<false, 4, 2, kInPack2>(),
-                                                      make_variant<false, 4, 2, kInPack3>()};
+// Forward kernels for the small / packed input forms: variant 3's shape (4
+// warps, 2 slots, stage-1 sums kept as int32 in shared memory; 3 CTAs/SM).
+static const Variant kFormVariants[kNumInputForms] = {
+    make_variant<false, 4, 2, kInSmall, false, OneSeg, true>(),
+    make_variant<false, 4, 2, kInPack2, false, OneSeg, true>(),
+    make_variant<false, 4, 2, kInPack3, false, OneSeg, true>()};
 
 static thread_local int g_last_encode_result = 0;
 

@@ -176,6 +176,31 @@ __device__ __forceinline__ void stage_m_small(const uint32_t (&a)[2][2], int32_t
   *(uint32_t*)(row + w_odd + 256) = pack2(y0[3], y1[3]);
 }
 
+// stage_m_small without the reduction (the "wide" kernels): the sums S (below
+// 2^24: one data byte x + 128 per coefficient) go to the int32 intermediate
+// row as stage_m_wide stores them.
+__device__ __forceinline__ void stage_m_small_wide(const uint32_t (&a)[2][2], int32_t c_lo,
+                                                   int32_t c_hi, uint32_t bt0, uint32_t bt1,
+                                                   uint8_t* irow, uint32_t w_e, uint32_t w_o) {
+  const int32_t cinit[4] = {c_lo, c_lo, c_hi, c_hi};
+  const int32_t zero[4] = {0, 0, 0, 0};
+  int32_t lo0[4], hi0[4], lo1[4], hi1[4];
+  mma_k16(lo0, a[0], bt0, cinit);
+  mma_k16(hi0, a[1], bt0, zero);
+  mma_k16(lo1, a[0], bt1, cinit);
+  mma_k16(hi1, a[1], bt1, zero);
+  uint32_t y0[4], y1[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    y0[e] = (uint32_t)lo0[e] + ((uint32_t)hi0[e] << 7);
+    y1[e] = (uint32_t)lo1[e] + ((uint32_t)hi1[e] << 7);
+  }
+  *(uint2*)(irow + w_e) = make_uint2(y0[0], y1[0]);
+  *(uint2*)(irow + w_o) = make_uint2(y0[1], y1[1]);
+  *(uint2*)(irow + w_e + 512) = make_uint2(y0[2], y1[2]);
+  *(uint2*)(irow + w_o + 512) = make_uint2(y0[3], y1[3]);
+}
+
 // The single-limb B operands from stage_m's two k32 fragment registers of one
 // n-tile (int16 inputs): low bytes, biased to x + 128.  *bad collects bits
 // where a high byte is not the sign extension of its low byte (input outside

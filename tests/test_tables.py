@@ -81,11 +81,12 @@ def test_kernel_model_extreme_rows(tk, oracle, wide):
     assert (canon(iv(x, wide=wide, fold=True)) == canon(oracle.invntt(ref_in))).all()
 
 
+@pytest.mark.parametrize("wide", [False, True], ids=["int16-mid", "int32-mid"])
 @pytest.mark.parametrize("lo,hi", [(-128, 128), (-3, 4), (-1, 2)])
-def test_single_limb_stage1_model(tk, oracle, lo, hi):
+def test_single_limb_stage1_model(tk, oracle, lo, hi, wide):
     """The single-limb stage-1 fragments (inputs in [-128, 127]) give the same
     transform as the reference's ntt, extremes included."""
     fw = KM.FwdModel(tk.get_table(4))
     x = rng(7 + hi).integers(lo, hi, size=(200, 256)).astype(np.int16)
     x[0], x[1] = lo, hi - 1
-    assert (fw(x, single_limb=True) == canon(oracle.ntt(x))).all()
+    assert (fw(x, single_limb=True, wide=wide) == canon(oracle.ntt(x))).all()
