@@ -182,3 +182,31 @@ def test_matvec_pipeline_every_variant(tk, cuda, oracle, variant):
         tk.set_variant(tk.INVERSE, -1)
         tk.set_option(tk.OPT_MATVEC_MODE, before)
     assert (canon(out) == canon(oracle_out(oracle, 3, A, s, e))).all()
+
+
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_matvec_tile_boundaries(tk, cuda, oracle, mode, k):
+    """Job counts on and around the tiled kernel's tile sizes (16 jobs for
+    k = 2, 8 for k = 3, 4) and around a whole first wave of CTAs: every job
+    equals the oracle, and the same jobs give the same bytes in every count."""
+    per = 16 if k == 2 else 8
+    A, s, e = make_jobs(90 + k, k, 8 * per + 1)
+    ref = oracle_out(oracle, k, A, s, e)
+    for n in (1, per - 1, per, per + 1, 8 * per + 1):
+        (out,) = run(tk, cuda, [(k, A[:n], s[:n], e[:n])])
+        assert (canon(out) == canon(ref[:n])).all(), n
+    assert tk.device_status(0) == 0
+
+
+def test_matvec_mixed_k_in_place_many_batches(tk, cuda, oracle, mode):
+    """Six batches of alternating k in one call (two launches of the tiled
+    kernel), in place, some without e: equal to the oracle."""
+    spec = [(4, 37, True), (2, 5, False), (3, 100, True), (4, 1, True), (2, 64, True), (3, 17, False)]
+    items = []
+    for i, (k, n, with_e) in enumerate(spec):
+        A, s, e = make_jobs(70 + i, k, n)
+        items.append((k, A, s, e if with_e else None))
+    outs = run(tk, cuda, items, inplace=True)
+    for (k, A, s, e), out in zip(items, outs):
+        assert (canon(out) == canon(oracle_out(oracle, k, A, s, e))).all()
+    assert tk.device_status(0) == 0
