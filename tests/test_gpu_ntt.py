@@ -182,6 +182,25 @@ def test_host_api_matches_device(tk, cuda, oracle):
     assert (canon(h) == canon(x.astype(np.int64) * 65536)).all()
 
 
+@pytest.mark.parametrize("chunk", [0, 1000, 4096, 5000])
+def test_host_api_chunk_schedules(tk, cuda, chunk):
+    """The host path's chunk schedule (growing from 4096 polynomials to the
+    chunk option and shrinking at the end) on sizes around its steps: equal
+    to the device path byte for byte, both directions."""
+    x = rng(57).integers(-32768, 32768, size=(70001, 256)).astype(np.int16)
+    tk.set_option(tk.OPT_HOST_CHUNK_POLYS, chunk)
+    try:
+        for n in (1, 4095, 4097, 8193, 12289, 32769, 70001):
+            h = x[:n].copy()
+            tk.ntt_host(h)
+            assert (h == gpu_fwd(tk, cuda, x[:n])).all(), (chunk, n)
+            g = x[:n].copy()
+            tk.invntt_host(g)
+            assert (g == gpu_inv(tk, cuda, x[:n])).all(), (chunk, n)
+    finally:
+        tk.set_option(tk.OPT_HOST_CHUNK_POLYS, 0)
+
+
 def test_non_default_stream_and_threads(tk, cuda, oracle):
     xs = [rng(20 + i).integers(0, Q, size=(777 + 100 * i, 256)).astype(np.int16) for i in range(4)]
     ts = [to_dev(cuda, x) for x in xs]
