@@ -832,13 +832,11 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
     if (P.e[b]) bulk_prefetch_l2(P.e[b] + (size_t)j0 * kb * 128, (uint32_t)nj * kb * 512u);
   };
 
-  // one tile of batch b (k = K), its s in the given slot
-  auto run_tile = [&](auto kc, int b, int tl, uint32_t slot, uint8_t* slotp) {
-    constexpr int K = decltype(kc)::value;
-    constexpr int NU = tile_units(K), kJobs = tile_jobs(K);
-    const int njobs = P.njobs[b], nvec = njobs * K, row0 = tl * 8 * NU;
-
-    // forward NTT of the s tile, in place
+  // A tile's three phases.  The NTT phases depend on the tile's unit count
+  // only (4 for k = 2, 4; 3 for k = 3), so k = 2 and k = 4 share their code.
+  // forward NTT of the s tile (in the given slot), in place
+  auto fwd_phase = [&](auto nc, uint32_t slot, uint8_t* slotp) {
+    constexpr int NU = decltype(nc)::value;
     if (warp < NU) {
       uint32_t fam[2][4];
       load_am(g_fwd.s1, fam);
@@ -848,16 +846,16 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
                         (int32_t)c1.x, (int32_t)c1.y, cbz, w_even, w_odd, 0, nullptr, 0, 0, 0);
     }
     cta_sync_named();
-    {
-      uint32_t fac[PP][2][2][2];
-      load_ac(g_fwd.s2, fac);
-      block_stage<false, W, PP, NU>(slot, slotp, blk0, ldc_fwd, stc_off, fac, zc);
-    }
-    if (lane == 0) bulk_wait_read<0>();  // the accumulators' last store has been read out
-    cta_sync_named();
-
-    // basemul-accumulate into the accumulator tile, one job per warp at a
-    // time, all k^2 loads of A issued first
+    uint32_t fac[PP][2][2][2];
+    load_ac(g_fwd.s2, fac);
+    block_stage<false, W, PP, NU>(slot, slotp, blk0, ldc_fwd, stc_off, fac, zc);
+  };
+  // basemul-accumulate into the accumulator tile, one job per warp at a
+  // time, all k^2 loads of A issued first
+  auto basemul_phase = [&](auto kc, int b, int tl, const uint8_t* slotp) {
+    constexpr int K = decltype(kc)::value;
+    constexpr int kJobs = tile_jobs(K);
+    const int njobs = P.njobs[b];
     for (int jl = warp; jl < kJobs; jl += W) {
       const int job = tl * kJobs + jl;
       if (job >= njobs) break;  // warp-uniform
@@ -874,9 +872,10 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
       for (int i = 0; i < K; i++)
         *(uint4*)(accp + (jl * K + i) * kRowBytes + 16 * lane) = basemul_row<K>(a[i], bv, zr);
     }
-    cta_sync_named();
-
-    // inverse NTT plus e on the accumulator tile, in place; then the store
+  };
+  // inverse NTT plus e on the accumulator tile, in place; then the store
+  auto inv_phase = [&](auto nc, int b, int row0, int nvec) {
+    constexpr int NU = decltype(nc)::value;
     {
       uint32_t iac[PP][2][2][2];
       load_ac(g_inv.sa, iac);
@@ -904,6 +903,8 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
     }
     if (lane == 0) bulk_commit();  // every lane-0 keeps one (possibly empty) group per tile
   };
+  using U3 = std::integral_constant<int, 3>;
+  using U4 = std::integral_constant<int, 4>;
 
   issue_load(0, 0);
   prefetch(0);
@@ -922,11 +923,24 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
       prefetch(k + 1);
     }
     const int t = (int)blockIdx.x + k * G, b = batch_of(t), tl = t - P.first_tile[b];
-    switch (P.k[b]) {  // CTA-uniform
-      case 2: run_tile(std::integral_constant<int, 2>{}, b, tl, slot, slotp); break;
-      case 3: run_tile(std::integral_constant<int, 3>{}, b, tl, slot, slotp); break;
-      default: run_tile(std::integral_constant<int, 4>{}, b, tl, slot, slotp); break;
+    const int kb = P.k[b];  // CTA-uniform
+    const int row0 = tl * 8 * tile_units(kb), nvec = P.njobs[b] * kb;
+    if (kb == 3)
+      fwd_phase(U3{}, slot, slotp);
+    else
+      fwd_phase(U4{}, slot, slotp);
+    if (lane == 0) bulk_wait_read<0>();  // the accumulators' last store has been read out
+    cta_sync_named();
+    switch (kb) {
+      case 2: basemul_phase(std::integral_constant<int, 2>{}, b, tl, slotp); break;
+      case 3: basemul_phase(std::integral_constant<int, 3>{}, b, tl, slotp); break;
+      default: basemul_phase(std::integral_constant<int, 4>{}, b, tl, slotp); break;
     }
+    cta_sync_named();
+    if (kb == 3)
+      inv_phase(U3{}, b, row0, nvec);
+    else
+      inv_phase(U4{}, b, row0, nvec);
   }
   if (lane == 0) bulk_wait_all();
 }
