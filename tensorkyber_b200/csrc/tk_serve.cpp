@@ -58,6 +58,9 @@ constexpr auto kSpinAfterWork = std::chrono::microseconds(2000);
 // the copy streams, so completions are never stuck behind a deep queue of
 // input copies (further requests wait, in order, on the host).
 constexpr size_t kMaxActive = 64;
+// input-copy streams (the copy engine's fixed cost per operation overlaps
+// across streams)
+constexpr int kCopyStreams = 3;
 // Under load, admission waits until this many slots under kMaxActive are free
 // and then admits them in one pass, published with a single stream write:
 // otherwise every freed slot would cost its own pass (copy + publish) on the
@@ -143,6 +146,13 @@ struct tk_server {
   uint32_t nslots = 0;
   std::vector<uint32_t> free_slots, slot_gen;
   cudaStream_t h2d = nullptr, d2h = nullptr, comp = nullptr;
+  // more input-copy streams: a pass's copies are dealt over h2d and these
+  // (the fixed cost of each copy operation overlaps), and the pass's tail
+  // write on h2d waits for all of them
+  cudaStream_t h2d_more[kCopyStreams - 1] = {};
+  cudaEvent_t copied[kCopyStreams - 1] = {};
+  unsigned pass_streams = 0;  // bit i: h2d_more[i] took a copy in this pass
+  unsigned next_stream = 0;
   cudaEvent_t kernel_done = nullptr;
   bool kernel_running = false;
   unsigned long long published = 0;  // jobs, full width on the host
@@ -242,14 +252,17 @@ cudaError_t admit(tk_server* S, Request* r) {
     int16_t* dA = (int16_t*)base;
     int16_t* ds = (int16_t*)(base + ab);
     int16_t* de = r->e ? (int16_t*)(base + ab + vb) : nullptr;
+    // this request's copies go to the next copy stream of the rotation
+    const unsigned k_st = S->next_stream++ % kCopyStreams;
+    cudaStream_t st = k_st == 0 ? S->h2d : S->h2d_more[k_st - 1];
+    if (k_st) S->pass_streams |= 1u << (k_st - 1);
     cudaError_t e;
     if (r->packed) {
-      e = cudaMemcpyAsync(dA, r->A, ab + vb * (r->e ? 2 : 1), cudaMemcpyHostToDevice, S->h2d);
+      e = cudaMemcpyAsync(dA, r->A, ab + vb * (r->e ? 2 : 1), cudaMemcpyHostToDevice, st);
     } else {
-      e = cudaMemcpyAsync(dA, r->A, ab, cudaMemcpyHostToDevice, S->h2d);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(ds, r->s, vb, cudaMemcpyHostToDevice, S->h2d);
-      if (e == cudaSuccess && de)
-        e = cudaMemcpyAsync(de, r->e, vb, cudaMemcpyHostToDevice, S->h2d);
+      e = cudaMemcpyAsync(dA, r->A, ab, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(ds, r->s, vb, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess && de) e = cudaMemcpyAsync(de, r->e, vb, cudaMemcpyHostToDevice, st);
     }
     if (e != cudaSuccess) return e;
     r->dA = dA;
@@ -280,6 +293,14 @@ cudaError_t admit(tk_server* S, Request* r) {
 // on the copy stream behind the input copies.
 cudaError_t publish(tk_server* S) {
   std::atomic_thread_fence(std::memory_order_seq_cst);  // descriptors before the doorbell
+  // the tail write waits for this pass's copies on the other copy streams
+  for (int i = 0; i < kCopyStreams - 1; i++) {
+    if (!(S->pass_streams & (1u << i))) continue;
+    cudaError_t e = cudaEventRecord(S->copied[i], S->h2d_more[i]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(S->h2d, S->copied[i], 0);
+    if (e != cudaSuccess) return e;
+  }
+  S->pass_streams = 0;
   return set_u32(&S->ctl->tail, (unsigned int)S->published, S->h2d);
 }
 
@@ -446,6 +467,13 @@ void scheduler(tk_server* S) {
 
 void destroy_resources(tk_server* S) {
   if (S->comp) cudaStreamSynchronize(S->comp);
+  for (int i = 0; i < kCopyStreams - 1; i++) {
+    if (S->h2d_more[i]) {
+      cudaStreamSynchronize(S->h2d_more[i]);
+      cudaStreamDestroy(S->h2d_more[i]);
+    }
+    if (S->copied[i]) cudaEventDestroy(S->copied[i]);
+  }
   if (S->kernel_done) cudaEventDestroy(S->kernel_done);
   if (S->h2d) cudaStreamDestroy(S->h2d);
   if (S->d2h) cudaStreamDestroy(S->d2h);
@@ -483,6 +511,10 @@ int tk_server_create(int device, const tk_server_config* cfg, tk_server** out) {
   cudaGetDevice(&prev);
   cudaSetDevice(device);
   cudaError_t e = cudaMalloc(&S->pool, budget);
+  for (int i = 0; i < kCopyStreams - 1 && e == cudaSuccess; i++) {
+    e = cudaStreamCreateWithFlags(&S->h2d_more[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->copied[i], cudaEventDisableTiming);
+  }
   if (e == cudaSuccess) e = cudaMalloc(&S->ctl, sizeof(tk::ServeCtl));
   if (e == cudaSuccess) e = cudaMemset(S->ctl, 0, sizeof(tk::ServeCtl));
   if (e == cudaSuccess) e = cudaMalloc(&S->req_ctr, slots * sizeof(unsigned int));
