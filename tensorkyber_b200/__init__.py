@@ -403,6 +403,11 @@ class Server:
         self.close()
 
 
+# Options (tk_set_option): the pipeline mode's chunk in vector polynomials,
+# the host path's largest chunk in polynomials, and the matrix-vector mode:
+# MATVEC_TILED (the default: one kernel, a CTA per tile of 8-16 jobs),
+# MATVEC_PIPELINE (NTT, basemul-accumulate, iNTT + e as three kernels per
+# chunk) or MATVEC_FUSED (one kernel, one warp per job).
 OPT_MATVEC_CHUNK_POLYS = 1
 OPT_HOST_CHUNK_POLYS = 3
 OPT_MATVEC_MODE = 2
