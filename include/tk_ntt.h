@@ -272,6 +272,9 @@ int tk_abi_version(void);
  *   0: M1[16][16]   1: M2[16][16][16]   2: MA[16][16][16]   3: Minv[16][16]
  *      (int16 residues in [0, q), see tensorkyber_b200/csrc/tk_tables.h)
  *   4: forward fragment tables   5: inverse fragment tables
+ *   6: basemul pair constants int32[128], z_t * 2^-16 mod q with
+ *      z_t = +-17^brv7(64 + t/2) (+ for even t), as the matrix-vector
+ *      kernels upload them
  * Copies min(bytes, size) bytes to out and returns the table size in bytes,
  * or -TK_ERR_INVALID_VALUE.  Counterpart of setup_tc_matrices
  * (ntt_bench/ntt_kernels.cuh:842-925), which builds the same maps. */

@@ -1009,11 +1009,13 @@ long long tk_get_table(int which, void* out, size_t bytes) {
   static tk::Matrices M;
   static tk::FwdFrags FF;
   static tk::InvFrags IF;
+  static int32_t ZR[128];
   static std::once_flag once;
   std::call_once(once, [] {
     tk::build_matrices(&M);
     tk::build_fwd_frags(M, &FF);
     tk::build_inv_frags(M, &IF);
+    tk::build_pair_constants(ZR);
   });
   const void* src;
   size_t size;
@@ -1024,6 +1026,7 @@ long long tk_get_table(int which, void* out, size_t bytes) {
     case 3: src = M.minv; size = sizeof(M.minv); break;
     case 4: src = &FF; size = sizeof(FF); break;
     case 5: src = &IF; size = sizeof(IF); break;
+    case 6: src = ZR; size = sizeof(ZR); break;
     default: return -TK_ERR_INVALID_VALUE;
   }
   if (out) memcpy(out, src, bytes < size ? bytes : size);
