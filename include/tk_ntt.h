@@ -275,6 +275,8 @@ int tk_abi_version(void);
  *   6: basemul pair constants int32[128], z_t * 2^-16 mod q with
  *      z_t = +-17^brv7(64 + t/2) (+ for even t), as the matrix-vector
  *      kernels upload them
+ *   7: the tiled matrix-vector kernel's inverse fragment tables (layout of
+ *      5), computing 2^-16 * invntt
  * Copies min(bytes, size) bytes to out and returns the table size in bytes,
  * or -TK_ERR_INVALID_VALUE.  Counterpart of setup_tc_matrices
  * (ntt_bench/ntt_kernels.cuh:842-925), which builds the same maps. */

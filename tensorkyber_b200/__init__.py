@@ -171,7 +171,8 @@ _TABLE_SHAPES = {0: (16, 16), 1: (16, 16, 16), 2: (16, 16, 16), 3: (16, 16)}
 def get_table(which: int) -> np.ndarray:
     """Host matrix builder output (no GPU needed): 0 M1, 1 M2, 2 MA, 3 Minv as
     int16 residues; 4 / 5 the forward / inverse fragment tables as raw uint32;
-    6 the basemul pair constants as int32[128]."""
+    6 the basemul pair constants as int32[128]; 7 the tiled matrix-vector
+    kernel's inverse fragment tables (2^-16 * invntt) as raw uint32."""
     L = lib()
     size = L.tk_get_table(which, None, 0)
     if size < 0:

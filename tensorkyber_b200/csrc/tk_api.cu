@@ -1008,7 +1008,7 @@ int tk_autotune_reset(void) {
 long long tk_get_table(int which, void* out, size_t bytes) {
   static tk::Matrices M;
   static tk::FwdFrags FF;
-  static tk::InvFrags IF;
+  static tk::InvFrags IF, IFR;
   static int32_t ZR[128];
   static std::once_flag once;
   std::call_once(once, [] {
@@ -1016,6 +1016,9 @@ long long tk_get_table(int which, void* out, size_t bytes) {
     tk::build_fwd_frags(M, &FF);
     tk::build_inv_frags(M, &IF);
     tk::build_pair_constants(ZR);
+    tk::Matrices MR = M;
+    tk::scale_inverse(&MR, 169);  // 2^-16 mod q
+    tk::build_inv_frags(MR, &IFR);
   });
   const void* src;
   size_t size;
@@ -1027,6 +1030,7 @@ long long tk_get_table(int which, void* out, size_t bytes) {
     case 4: src = &FF; size = sizeof(FF); break;
     case 5: src = &IF; size = sizeof(IF); break;
     case 6: src = ZR; size = sizeof(ZR); break;
+    case 7: src = &IFR; size = sizeof(IFR); break;
     default: return -TK_ERR_INVALID_VALUE;
   }
   if (out) memcpy(out, src, bytes < size ? bytes : size);

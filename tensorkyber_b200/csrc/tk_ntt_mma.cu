@@ -724,7 +724,10 @@ struct MvTiles {
   int nb;
 };
 
-__device__ int32_t g_tile_zr[128];  // basemul pair constants (build_pair_constants)
+__device__ int32_t g_tile_z[128];  // basemul pair roots z_t (build_pair_roots)
+// The tiled kernel's inverse: g_inv with stage B scaled by 2^-16, the factor
+// its basemul leaves out (basemul_row_z).
+__device__ InvFrags g_tile_inv;
 
 constexpr int kTileSlotBytes = 32 * kRowBytes;      // one 32-row slot
 constexpr int kTileSmem = 3 * kTileSlotBytes + 16;  // s slot x 2, accumulators, 2 mbarriers
@@ -777,9 +780,9 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
           ac[p][h][s][1] = v.y;
         }
   };
-  uint32_t zr[4];
+  uint32_t zt[4];
 #pragma unroll
-  for (int u = 0; u < 4; u++) zr[u] = (uint32_t)g_tile_zr[4 * lane + u];
+  for (int u = 0; u < 4; u++) zt[u] = (uint32_t)g_tile_z[4 * lane + u];
 
   if (tid == 0) {
     mbar_init(bar0, W);
@@ -861,16 +864,19 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
       if (job >= njobs) break;  // warp-uniform
       const int16_t* Aj = P.A[b] + (size_t)job * K * K * 256 + 8 * lane;
       uint4 a[K][K], bv[K];
+      uint2 zb[K];
 #pragma unroll
       for (int i = 0; i < K; i++)
 #pragma unroll
         for (int j = 0; j < K; j++) a[i][j] = __ldcs((const uint4*)(Aj + (i * K + j) * 256));
 #pragma unroll
-      for (int j = 0; j < K; j++)
+      for (int j = 0; j < K; j++) {
         bv[j] = *(const uint4*)(slotp + (jl * K + j) * kRowBytes + 16 * lane);
+        zb[j] = pair_zb(bv[j], zt);
+      }
 #pragma unroll
       for (int i = 0; i < K; i++)
-        *(uint4*)(accp + (jl * K + i) * kRowBytes + 16 * lane) = basemul_row<K>(a[i], bv, zr);
+        *(uint4*)(accp + (jl * K + i) * kRowBytes + 16 * lane) = basemul_row_z<K>(a[i], bv, zb);
     }
   };
   // inverse NTT plus e on the accumulator tile, in place; then the store
@@ -884,11 +890,11 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
     cta_sync_named();
     if (warp < NU) {
       uint32_t iam[2][4];
-      load_am(g_inv.sb, iam);
+      load_am(g_tile_inv.sb, iam);
       int32_t cb[2][4];
 #pragma unroll
       for (int t = 0; t < 2; t++) {
-        const uint4 v = ldg_keep_u4(&g_inv.cbz[lane][t][0]);
+        const uint4 v = ldg_keep_u4(&g_tile_inv.cbz[lane][t][0]);
         cb[t][0] = (int32_t)v.x;
         cb[t][1] = (int32_t)v.y;
         cb[t][2] = (int32_t)v.z;
@@ -1047,20 +1053,24 @@ static bool encode_packed_map(CUtensorMap* map, const void* base, int npoly, int
 int last_encode_result() { return g_last_encode_result; }
 
 static bool upload_tables_current_device() {
-  static Matrices M;
+  static Matrices M, MR;
   static FwdFrags FF;
-  static InvFrags IF;
+  static InvFrags IF, IFR;
   static std::once_flag once;
   std::call_once(once, [] {
     build_matrices(&M);
     build_fwd_frags(M, &FF);
     build_inv_frags(M, &IF);
+    MR = M;
+    scale_inverse(&MR, kRinv);
+    build_inv_frags(MR, &IFR);
   });
   if (cudaMemcpyToSymbol(g_fwd, &FF, sizeof(FF)) != cudaSuccess) return false;
   if (cudaMemcpyToSymbol(g_inv, &IF, sizeof(IF)) != cudaSuccess) return false;
-  int32_t zr[128];
-  build_pair_constants(zr);
-  if (cudaMemcpyToSymbol(g_tile_zr, zr, sizeof(zr)) != cudaSuccess) return false;
+  if (cudaMemcpyToSymbol(g_tile_inv, &IFR, sizeof(IFR)) != cudaSuccess) return false;
+  int32_t z[128];
+  build_pair_roots(z);
+  if (cudaMemcpyToSymbol(g_tile_z, z, sizeof(z)) != cudaSuccess) return false;
   const unsigned zero = 0;
   return cudaMemcpyToSymbol(g_status, &zero, sizeof(zero)) == cudaSuccess;
 }

@@ -348,4 +348,43 @@ __device__ __forceinline__ uint4 basemul_row(const uint4 (&a)[K], const uint4 (&
   return make_uint4(o[0], o[1], o[2], o[3]);
 }
 
+// The same products with z folded into ntt(s) and 2^-16 left to the caller
+// (the tiled kernel's inverse tables carry it).  zb = the lane's z_t * b1
+// for its four pairs of one polynomial (b1 in [0, q)), as 16-bit values in
+// [0, q + 4): red_wide of a product below q^2 is off by less than 0.002 q.
+__device__ __forceinline__ uint2 pair_zb(const uint4 b, const uint32_t (&z)[4]) {
+  const uint32_t p0 = red_wide((b.x >> 16) * z[0]), p1 = red_wide((b.y >> 16) * z[1]);
+  const uint32_t p2 = red_wide((b.z >> 16) * z[2]), p3 = red_wide((b.w >> 16) * z[3]);
+  return make_uint2(p0 | (p1 << 16), p2 | (p3 << 16));
+}
+
+constexpr uint32_t kSumBiasZ = 3329u << 19;  // >= |sum| (< 2^29.71); sum + bias < 2^32
+
+// Per pair, out0 = sum_j a0 b0 + a1 (z b1), out1 = sum_j a0 b1 + a1 b0, each
+// reduced once: 2^16 times the reference's basemul-accumulate, mod q.  With
+// b0, b1 < q and z b1 < q + 4, |sum| <= 2K * 32768 * (q + 3) < 2^29.71 for
+// K <= 4, so the biased sums lie in [0, 2^32) and red_wide leaves [0, 1.41 q).
+template <int K>
+__device__ __forceinline__ uint4 basemul_row_z(const uint4 (&a)[K], const uint4 (&b)[K],
+                                               const uint2 (&zb)[K]) {
+  uint32_t o[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    uint32_t t0 = kSumBiasZ, t1 = kSumBiasZ;
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+      const uint32_t aw = u == 0 ? a[j].x : u == 1 ? a[j].y : u == 2 ? a[j].z : a[j].w;
+      const uint32_t bw = u == 0 ? b[j].x : u == 1 ? b[j].y : u == 2 ? b[j].z : b[j].w;
+      const uint32_t zw = u < 2 ? zb[j].x : zb[j].y;
+      const int32_t a0 = (int16_t)(aw & 0xffffu), a1 = (int32_t)aw >> 16;
+      const int32_t b0 = (int32_t)(bw & 0xffffu), b1 = (int32_t)(bw >> 16);
+      const int32_t z1 = (int32_t)((u & 1) ? zw >> 16 : zw & 0xffffu);
+      t0 += (uint32_t)(a0 * b0 + a1 * z1);
+      t1 += (uint32_t)(a0 * b1 + a1 * b0);
+    }
+    o[u] = pack2(red_wide(t0), red_wide(t1));
+  }
+  return make_uint4(o[0], o[1], o[2], o[3]);
+}
+
 }  // namespace tk

@@ -82,13 +82,22 @@ int64_t byte_weighted(int64_t c, int byte) {
 
 }  // namespace
 
+void build_pair_roots(int32_t z[128]) {
+  for (int t = 0; t < 128; t++) {
+    const int64_t w = tw().w[64 + t / 2];
+    z[t] = (int32_t)((t & 1) ? modq(-w) : w);
+  }
+}
+
 void build_pair_constants(int32_t zr[128]) {
   const int64_t rinv = 169;  // 2^-16 mod q
-  for (int t = 0; t < 128; t++) {
-    int64_t z = tw().w[64 + t / 2];
-    if (t & 1) z = modq(-z);
-    zr[t] = (int32_t)(z * rinv % kQ);
-  }
+  build_pair_roots(zr);
+  for (int t = 0; t < 128; t++) zr[t] = (int32_t)(zr[t] * rinv % kQ);
+}
+
+void scale_inverse(Matrices* M, int64_t f) {
+  for (int i = 0; i < 16; i++)
+    for (int m = 0; m < 16; m++) M->minv[i][m] = (int16_t)modq(M->minv[i][m] * f);
 }
 
 void build_matrices(Matrices* M) {

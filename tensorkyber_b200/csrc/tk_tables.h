@@ -115,6 +115,12 @@ struct Matrices {
 // is the residue mod X^2 - z_t, z_t = +-17^brv7(64 + t/2) (sign + for even t);
 // zr[t] = z_t * 2^-16 mod q (the reference's basemul multiplies by 2^-16).
 void build_pair_constants(int32_t zr[128]);
+// z[t] = z_t itself, in [0, q).
+void build_pair_roots(int32_t z[128]);
+
+// Scales the inverse transform by f (mod q): Minv <- f * Minv, so that tables
+// built from M compute f * invntt.
+void scale_inverse(Matrices* M, int64_t f);
 
 void build_matrices(Matrices* M);
 void build_fwd_frags(const Matrices& M, FwdFrags* F);

@@ -87,7 +87,8 @@ def test_get_table_sizes(tk):
     assert L.tk_get_table(0, None, 0) == 16 * 16 * 2
     assert L.tk_get_table(1, None, 0) == 16 * 16 * 16 * 2
     assert L.tk_get_table(6, None, 0) == 128 * 4
-    assert L.tk_get_table(7, None, 0) < 0
+    assert L.tk_get_table(7, None, 0) == L.tk_get_table(5, None, 0)
+    assert L.tk_get_table(8, None, 0) < 0
     assert L.tk_get_table(-1, None, 0) < 0
     small = (ctypes.c_uint8 * 4)()
     assert L.tk_get_table(0, small, 4) == 512                 # truncating copy is allowed

@@ -1,12 +1,19 @@
-"""CPU model of the kernels' basemul-accumulate arithmetic (basemul_row in
-tk_stages.cuh, used by the tiled matrix-vector kernel and the pipeline's
-basemul kernel), checked against the oracle's composition of the reference's
-basemul (ntt_bench/ref/ntt.c:139-146, applied pairwise as ML-KEM's
-poly_basemul_montgomery).  Integer work, no GPU: every intermediate bound the
-kernels rely on is asserted, on random and extreme inputs."""
+"""CPU model of the kernels' basemul-accumulate arithmetic, checked against
+the oracle's composition of the reference's basemul (ntt_bench/ref/ntt.c:139-146,
+applied pairwise as ML-KEM's poly_basemul_montgomery):
+
+* basemul_row (tk_stages.cuh, the pipeline's basemul kernel): three raw sums
+  per pair, the pair constant z_t * 2^-16 applied after the sum;
+* basemul_row_z with pair_zb (the tiled matrix-vector kernel): z_t folded
+  into ntt(s) once per polynomial, two raw sums per pair, and 2^-16 left to
+  the inverse tables that kernel uses (table 7).
+
+Integer work, no GPU: every intermediate bound the kernels rely on is
+asserted, on random and extreme inputs."""
 import numpy as np
 import pytest
 
+import kernel_model as KM
 from conftest import rng
 from py_oracle import Q, canon
 
@@ -17,6 +24,15 @@ SUM_BIAS = 3329 * 262144      # the raw sums' bias (>= their magnitude)
 
 def brv7(x):
     return int(format(x, "07b")[::-1], 2)
+
+
+def pair_roots():
+    """z_t = 17^brv7(64 + t/2), negated for odd t."""
+    z = np.zeros(128, dtype=np.int64)
+    for t in range(128):
+        w = pow(17, brv7(64 + t // 2), Q)
+        z[t] = (-w) % Q if t & 1 else w
+    return z
 
 
 def pair_constants():
@@ -59,6 +75,95 @@ def basemul_row_model(a, b, zr):
 def test_pair_constants_match_library(tk):
     """The table the matrix-vector kernels upload is the one modelled here."""
     assert (tk.get_table(6).astype(np.int64) == pair_constants()).all()
+
+
+SUM_BIAS_Z = 3329 << 19
+
+
+def pair_zb_model(b, z):
+    """b: (K, 256) in [0, q); returns z_t * b1 per pair, (K, 128), lazily reduced."""
+    b1 = b.astype(np.int64).reshape(-1, 128, 2)[..., 1]
+    zb = red_wide(b1 * z)
+    assert zb.max() < Q + 4
+    return zb
+
+
+def basemul_row_z_model(a, b, zb):
+    """2^16 * sum_j basemul(A_ij, b_j) mod q, values in [0, 1.41 q)."""
+    a = a.astype(np.int64).reshape(-1, 128, 2)
+    b = b.astype(np.int64).reshape(-1, 128, 2)
+    assert b.min() >= 0 and b.max() < Q
+    t0 = (a[..., 0] * b[..., 0] + a[..., 1] * zb).sum(0)
+    t1 = (a[..., 0] * b[..., 1] + a[..., 1] * b[..., 0]).sum(0)
+    out = []
+    for t in (t0, t1):
+        assert np.abs(t).max() <= SUM_BIAS_Z
+        s = t + SUM_BIAS_Z
+        assert s.min() >= 0 and s.max() < (1 << 32)        # uint32 accumulator
+        r = s - ((s * BAR_LAZY) >> 32) * Q
+        assert r.min() >= 0 and r.max() < 4682                # [0, 1.41 q)
+        out.append(r)
+    return np.stack(out, axis=1).reshape(256)
+
+
+def test_pair_roots_match_library(tk):
+    assert (pair_roots() * RINV % Q == tk.get_table(6)).all()
+
+
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_basemul_row_z_model_matches_oracle(oracle, k):
+    z = pair_roots()
+    r = rng(500 + k)
+    for trial in range(20):
+        A = r.integers(-32768, 32768, size=(k, k, 256)).astype(np.int16)
+        b = r.integers(0, Q, size=(k, 256)).astype(np.int16)
+        zb = pair_zb_model(b, z)
+        for i in range(k):
+            ref = np.zeros(256, dtype=np.int64)
+            for j in range(k):
+                ref += oracle.poly_basemul(A[i, j], b[j]).astype(np.int64)
+            got = basemul_row_z_model(A[i], b, zb) * RINV
+            assert (canon(got) == canon(ref)).all(), (trial, i)
+
+
+@pytest.mark.parametrize("aval", [-32768, 32767])
+@pytest.mark.parametrize("bval", [Q - 1, 0, 1])
+def test_basemul_row_z_model_extremes(oracle, aval, bval):
+    """k = 4, every A coefficient at an int16 extreme, ntt(s) constant: the
+    raw sums reach their largest magnitude."""
+    k = 4
+    z = pair_roots()
+    A = np.full((k, k, 256), aval, dtype=np.int16)
+    A[:, :, 1::2] = -1 - aval if bval == 0 else aval        # a1 of the other sign too
+    b = np.full((k, 256), bval, dtype=np.int16)
+    b[:, 1::2] = Q - 1
+    zb = pair_zb_model(b, z)
+    ref = np.zeros(256, dtype=np.int64)
+    for j in range(k):
+        ref += oracle.poly_basemul(A[0, j], b[j]).astype(np.int64)
+    assert (canon(basemul_row_z_model(A[0], b, zb) * RINV) == canon(ref)).all()
+
+
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_tiled_job_model_matches_oracle(tk, oracle, k):
+    """One job of the tiled kernel on the CPU: the forward model on the
+    library's tables, basemul_row_z, the inverse model on table 7 (stage B
+    scaled by 2^-16, bias folded into its init), then + e with int16
+    wrap-around, against the oracle's job."""
+    fw = KM.FwdModel(tk.get_table(4))
+    iv = KM.InvModel(tk.get_table(7))
+    z = pair_roots()
+    r = rng(600 + k)
+    for trial in range(4):
+        A = r.integers(-32768, 32768, size=(k, k, 256)).astype(np.int16)
+        s = r.integers(-3, 4, size=(k, 256)).astype(np.int16)
+        e = r.integers(-3, 4, size=(k, 256)).astype(np.int16)
+        b = fw(s)
+        zb = pair_zb_model(b, z)
+        acc = np.stack([basemul_row_z_model(A[i], b, zb) for i in range(k)]).astype(np.int16)
+        v = iv(acc, fold=True)
+        out = (v.astype(np.int64) + e).astype(np.int16)
+        assert (canon(out) == canon(oracle.matvec_job(k, A, s, e))).all(), trial
 
 
 @pytest.mark.parametrize("k", [2, 3, 4])
