@@ -6,7 +6,10 @@ applied pairwise as ML-KEM's poly_basemul_montgomery):
   per pair, the pair constant z_t * 2^-16 applied after the sum;
 * basemul_row_z with pair_zb (the tiled matrix-vector kernel): z_t folded
   into ntt(s) once per polynomial, two raw sums per pair, and 2^-16 left to
-  the inverse tables that kernel uses (table 7).
+  the inverse tables that kernel uses (table 7);
+* fused_job's products (tk_matvec.cu, the fused kernel and the server's
+  device loop): 2^-16 and z_t both folded into ntt(s), lazily reduced, with
+  the accumulator bias kAccBias.
 
 Integer work, no GPU: every intermediate bound the kernels rely on is
 asserted, on random and extreme inputs."""
@@ -164,6 +167,71 @@ def test_tiled_job_model_matches_oracle(tk, oracle, k):
         v = iv(acc, fold=True)
         out = (v.astype(np.int64) + e).astype(np.int16)
         assert (canon(out) == canon(oracle.matvec_job(k, A, s, e))).all(), trial
+
+
+ACC_BIAS = 1073742318          # q * ceil(2^30 / q)
+
+
+def fused_job_basemul_model(a, b, zr):
+    """fused_job step 4 for one output row: B0 = b0 * 2^-16, B1 = b1 * 2^-16,
+    Bz = b1 * z_t 2^-16, each lazily reduced (mulmod_lazy); int32 accumulators
+    biased by kAccBias, reduced once.  Equals the reference's basemul sum mod q."""
+    b = b.astype(np.int64).reshape(-1, 128, 2)
+    a = a.astype(np.int64).reshape(-1, 128, 2)
+    assert b.min() >= 0 and b.max() < Q              # forward stage 2 output
+
+    def lazy(x):                                        # red_lazy, x < 2^24
+        assert x.min() >= 0 and x.max() < (1 << 24)
+        r = x - ((x * BAR_LAZY) >> 32) * Q
+        assert r.max() < Q + 8
+        return r
+    B0, B1, Bz = lazy(b[..., 0] * RINV), lazy(b[..., 1] * RINV), lazy(b[..., 1] * zr)
+    acc0 = (a[..., 0] * B0 + a[..., 1] * Bz).sum(0)
+    acc1 = (a[..., 0] * B1 + a[..., 1] * B0).sum(0)
+    out = []
+    for acc in (acc0, acc1):
+        assert np.abs(acc).max() < (1 << 31) and np.abs(acc).max() <= ACC_BIAS
+        s = acc + ACC_BIAS
+        assert s.min() >= 0 and s.max() < (1 << 31)
+        out.append(red_wide(s))
+    r = np.stack(out, axis=1).reshape(256)
+    assert r.max() < (1 << 15)                          # int16 row for the inverse
+    return r
+
+
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_fused_job_basemul_model_matches_oracle(oracle, k):
+    zr = pair_constants()
+    r = rng(700 + k)
+    for trial in range(10):
+        A = r.integers(-32768, 32768, size=(k, k, 256)).astype(np.int16)
+        b = r.integers(0, Q, size=(k, 256)).astype(np.int16)
+        for i in range(k):
+            ref = np.zeros(256, dtype=np.int64)
+            for j in range(k):
+                ref += oracle.poly_basemul(A[i, j], b[j]).astype(np.int64)
+            assert (canon(fused_job_basemul_model(A[i], b, zr)) == canon(ref)).all(), (trial, i)
+
+
+@pytest.mark.parametrize("aval", [-32768, 32767])
+def test_fused_job_basemul_model_extremes(oracle, aval):
+    """k = 4, A at an int16 extreme, ntt(s) chosen so every lazy product lands
+    at the top of its range: the accumulators reach their largest magnitude."""
+    k = 4
+    zr = pair_constants()
+    A = np.full((k, k, 256), aval, dtype=np.int16)
+    v = np.arange(Q, dtype=np.int64)
+
+    def lazy_argmax(c):                                  # the b maximising red_lazy(b * c)
+        x = v * c
+        return int(np.argmax(x - ((x * BAR_LAZY) >> 32) * Q))
+    worst = np.zeros((k, 256), dtype=np.int16)
+    worst[:, 0::2] = lazy_argmax(RINV)
+    worst[:, 1::2] = [lazy_argmax(int(c)) for c in zr]
+    ref = np.zeros(256, dtype=np.int64)
+    for j in range(k):
+        ref += oracle.poly_basemul(A[0, j], worst[j]).astype(np.int64)
+    assert (canon(fused_job_basemul_model(A[0], worst, zr)) == canon(ref)).all()
 
 
 @pytest.mark.parametrize("k", [2, 3, 4])
