@@ -69,6 +69,30 @@ def test_matvec_no_addend_in_place_and_wide_inputs(tk, cuda, oracle, mode):
     assert (canon(out) == canon(ref)).all()
 
 
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_matvec_full_int16_A_and_extremes(tk, cuda, oracle, mode, k):
+    """A over the full int16 range, plus jobs whose A is all -32768 or all
+    32767, s over the full int16 range (the worst-case sums themselves are
+    pinned by the CPU models of the basemul arithmetic).  The oracle's job
+    adds its k basemul terms in int16, which can wrap for such A (a term
+    reaches ~30,000 when ntt(s) nears its 8q bound), so the reference here is
+    its primitives with the sum taken exactly: each basemul, on ntt(s) reduced
+    to [0, q), stays in int16 for any int16 A."""
+    A, _, e = make_jobs(40 + k, k, 40, a_lo=-32768, a_hi=32768)
+    A[0], A[1] = -32768, 32767
+    s = rng(50 + k).integers(-32768, 32768, size=e.shape).astype(np.int16)
+    (out,) = run(tk, cuda, [(k, A, s, e)])
+    n = A.shape[0]
+    # the oracle's ntt overflows int16 outside |x| <= 9471: feed it canon(s)
+    b = canon(oracle.ntt(canon(s).reshape(-1, 256))).reshape(n, k, 256)
+    ref = np.zeros((n, k, 256), dtype=np.int64)
+    for t in range(n):
+        for i in range(k):
+            acc = sum(oracle.poly_basemul(A[t, i, j], b[t, j]).astype(np.int64) for j in range(k))
+            ref[t, i] = oracle.invntt(canon(acc)[None])[0].astype(np.int64) + e[t, i]
+    assert (canon(out) == canon(ref)).all()
+
+
 def test_matvec_spans_several_chunks(tk, cuda, oracle, mode):
     """k = 2 with more jobs than one chunk (chunk set to 32768 vector polys)."""
     k, n = 2, 40000
