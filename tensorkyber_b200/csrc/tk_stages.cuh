@@ -309,7 +309,9 @@ __device__ __forceinline__ void stage_c_inv_wide(const uint32_t (&a)[2][2][2],
 constexpr uint32_t kRinv = 169;                 // 2^-16 mod q
 constexpr uint32_t kSumBias = 3329u * 262144u;  // > 2^29.7 >= |sum|; sum + bias < 2^31
 
-// S in [0, 2^31): representative in [0, 3q).
+// Any S < 2^32: representative in [0, 1.41 q) ([0, 1.21 q) for S < 2^31).
+// floor(S * 1290167 / 2^32) undershoots S / q by less than 0.41, so the
+// quotient is at most one below floor(S / q).
 __device__ __forceinline__ uint32_t red_wide(uint32_t s) {
   return s - __umulhi(s, 1290167u) * 3329u;
 }

@@ -75,6 +75,21 @@ def basemul_row_model(a, b, zr):
     return out
 
 
+def test_red_wide_bounds():
+    """red_wide on any uint32: the residue is kept and the representative lies
+    in [0, 1.41 q) ([0, 1.21 q) below 2^31), random and top-of-range values,
+    including every q j - 1 near 2^32."""
+    top = 1 << 32
+    s = np.concatenate([rng(9).integers(0, top, 1 << 20, dtype=np.int64),
+                        np.arange(top - (1 << 20), top, dtype=np.int64),
+                        Q * np.arange(top // Q - 4096, top // Q + 1, dtype=np.int64) - 1])
+    s = s[(s >= 0) & (s < top)]
+    r = s - ((s * BAR_LAZY) >> 32) * Q
+    assert (r % Q == s % Q).all() and r.min() >= 0 and r.max() < 1.41 * Q
+    low = s < (1 << 31)
+    assert r[low].max() < 1.21 * Q
+
+
 def test_pair_constants_match_library(tk):
     """The table the matrix-vector kernels upload is the one modelled here."""
     assert (tk.get_table(6).astype(np.int64) == pair_constants()).all()
