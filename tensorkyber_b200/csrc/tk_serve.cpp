@@ -44,6 +44,7 @@
 
 #include "../../include/tk_ntt.h"
 #include "tk_internal.h"
+#include "tk_pool.h"
 
 namespace {
 
@@ -91,44 +92,6 @@ struct Request {
   Clock::time_point t_submit, t_admit, t_flag, t_done;
 };
 
-// First-fit allocator over [0, size).
-class Pool {
- public:
-  void init(size_t n) {
-    free_.clear();
-    free_[0] = n;
-  }
-  bool alloc(size_t n, size_t* off) {
-    for (auto it = free_.begin(); it != free_.end(); ++it) {
-      if (it->second < n) continue;
-      *off = it->first;
-      const size_t rest = it->second - n, o = it->first;
-      free_.erase(it);
-      if (rest) free_[o + n] = rest;
-      return true;
-    }
-    return false;
-  }
-  void release(size_t off, size_t n) {
-    auto it = free_.emplace(off, n).first;
-    auto nx = std::next(it);
-    if (nx != free_.end() && it->first + it->second == nx->first) {
-      it->second += nx->second;
-      free_.erase(nx);
-    }
-    if (it != free_.begin()) {
-      auto pv = std::prev(it);
-      if (pv->first + pv->second == it->first) {
-        pv->second += it->second;
-        free_.erase(it);
-      }
-    }
-  }
-
- private:
-  std::map<size_t, size_t> free_;
-};
-
 }  // namespace
 
 struct tk_server {
@@ -137,7 +100,7 @@ struct tk_server {
   size_t budget = 0;
   bool zero_copy = false;
   uint8_t* pool = nullptr;
-  Pool alloc;
+  tk::Pool alloc;
   tk::ServeJob* ring = nullptr;       // job ring, mapped pinned host memory
   tk::ServeCtl* ctl = nullptr;
   unsigned int* req_ctr = nullptr;    // device
