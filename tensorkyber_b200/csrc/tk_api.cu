@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/tk_ntt.h"
+#include "tk_host_sched.h"
 #include "tk_internal.h"
 #include "tk_tables.h"
 
@@ -210,23 +211,13 @@ int run_device(bool inverse, const int16_t* in, int16_t* out, size_t npoly, cuda
   return TK_SUCCESS;
 }
 
-// Host path: chunks of at most stage_polys polynomials rotate through
-// kHostStages device buffers and streams, so the H2D copy of chunk c+1, the
-// kernel of chunk c and the D2H copy of chunk c-1 overlap, and an upload
-// waits only for the download kHostStages chunks back.  The first chunks grow
-// from kHostRampPolys and the last ones shrink to it: the first upload and the
-// last download run with nothing beside them, so they are kept short.
-constexpr size_t kHostRampPolys = 4096;
+// Host path: chunks of at most stage_polys polynomials (sized by
+// tk::host_chunk_size) rotate through kHostStages device buffers and streams,
+// so the H2D copy of chunk c+1, the kernel of chunk c and the D2H copy of
+// chunk c-1 overlap, and an upload waits only for the download kHostStages
+// chunks back.
 constexpr int kHostStages = 3;  // 4 measured the same
-size_t host_chunk_size(int c, size_t remaining, size_t chunk) {
-  size_t n = chunk;
-  if (c < 16 && (kHostRampPolys << c) < n) n = kHostRampPolys << c;
-  const size_t half = (remaining + 1) / 2;
-  const size_t tail = half > kHostRampPolys ? half : kHostRampPolys;
-  if (tail < n) n = tail;
-  if (remaining - n < kHostRampPolys && remaining <= chunk) n = remaining;  // no sliver
-  return n < remaining ? n : remaining;
-}
+using tk::host_chunk_size;
 int run_host(bool inverse, int16_t* polys, size_t npoly) {
   t_err[0] = 0;
   if (npoly == 0) return TK_SUCCESS;
