@@ -127,6 +127,15 @@ def test_matvec_job_composition(oracle):
             assert (canon(got[i]) == want).all()
 
 
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_matvec_job_golden(oracle, gold, k):
+    """tko_matvec_job, int16 for int16, against jobs that tests/golden/gen_golden.py
+    composed from the reference's own ntt, basemul, barrett_reduce and invntt."""
+    A, s, e, want = (gold[f"matvec{k}_{n}"] for n in ("A", "s", "e", "out"))
+    for t in range(A.shape[0]):
+        assert (oracle.matvec_job(k, A[t], s[t], e[t]) == want[t]).all(), t
+
+
 def test_pack_small_format(oracle):
     """TC-PACK byte layout (ntt_bench/ntt_bench.cu:744-752): coefficient i in
     byte i/(8/bits), field at bit (i % (8/bits))*bits, two's complement."""
