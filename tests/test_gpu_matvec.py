@@ -70,6 +70,16 @@ def test_matvec_no_addend_in_place_and_wide_inputs(tk, cuda, oracle, mode):
 
 
 @pytest.mark.parametrize("k", [2, 3, 4])
+def test_matvec_golden_reference_jobs(tk, cuda, golden, mode, k):
+    """The jobs that tests/golden/gen_golden.py composed from the reference's
+    own C functions, straight from the fixture (no oracle in between)."""
+    A = golden[f"matvec{k}_A"].reshape(-1, k, k, 256)
+    s, e, want = golden[f"matvec{k}_s"], golden[f"matvec{k}_e"], golden[f"matvec{k}_out"]
+    (out,) = run(tk, cuda, [(k, A, s, e)])
+    assert (canon(out) == canon(want)).all()
+
+
+@pytest.mark.parametrize("k", [2, 3, 4])
 def test_matvec_full_int16_A_and_extremes(tk, cuda, oracle, mode, k):
     """A over the full int16 range, plus jobs whose A is all -32768 or all
     32767, s over the full int16 range (the worst-case sums themselves are
