@@ -29,6 +29,32 @@ def test_reference_arm_prints_one_contract_line():
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["unit"] == d["unit"]
 
 
+def test_reference_arm_under_torchrun_two_ranks():
+    """Launched as the multi-GPU runs launch it: rank 0 alone measures and
+    prints one line, the other rank exits 0 without work."""
+    import signal
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port),
+           os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+           "--steps", "2", "--warmup", "1"]
+    p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True,
+                         cwd=ROOT, start_new_session=True)
+    try:
+        out, err = p.communicate(timeout=300)
+    except subprocess.TimeoutExpired:
+        os.killpg(p.pid, signal.SIGKILL)       # torchrun and both ranks
+        raise
+    assert p.returncode == 0, err[-2000:]
+    lines = [l for l in out.splitlines() if l.strip().startswith("{")]
+    assert len(lines) == 1, out
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+
+
 def test_default_arguments():
     sys.path.insert(0, ROOT)
     import bench
