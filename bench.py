@@ -12,9 +12,20 @@ L2 hygiene: four resident batches (4 x 128 MiB) rotate, so every launch reads
 a batch last touched three launches earlier (384 MiB of traffic in between,
 above the 126 MB L2).
 
+Timing: --repeats regions of exactly --steps steps each, every region
+bracketed by a barrier and a synchronize; the value is the median region (max
+over ranks), with min and max beside it.  --gpus N without a launcher starts N
+ranks itself through torch.distributed.run (one per GPU); under a launcher
+--gpus must equal the number of ranks.
+
+Beside the value (rank 0, one GPU): the reference's C on the host cores (all
+threads and one thread) and the reference's own GPU kernels on the same GPU
+(oracle/_ref/ntt_bench, built for sm_100a from ntt_bench/ntt_bench.cu).
+
 --impl reference times the reference's own C ntt()/invntt()
 (ntt_bench/ref, compiled unmodified into oracle/_ref) on all host threads, a
-4096-polynomial sample of the same workload per step.
+4096-polynomial sample of the same workload per step, in one process on rank
+0's host whatever --gpus is.
 """
 from __future__ import annotations
 
@@ -43,7 +54,11 @@ def parse():
     p.add_argument("--warmup", type=int, default=200)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--npoly", type=int, default=262144)
+    p.add_argument("--repeats", type=int, default=7,
+                   help="timed regions of --steps steps each; value = the median region")
     p.add_argument("--e2e-steps", type=int, default=30)
+    p.add_argument("--no-reference-gpu", action="store_true",
+                   help="skip the reference's own GPU kernels (oracle/_ref/ntt_bench)")
     p.add_argument("--cpu-seconds", type=float, default=6.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--variant", type=int, default=-1, help="force a kernel variant (-1: auto)")
@@ -165,12 +180,61 @@ def sample_input(n, seed=20240816):
 
 
 def cpu_baseline(seconds: float):
+    """The reference's C ntt() then invntt() on the host cores: all threads,
+    and one thread (its per-core rate)."""
     o, f, i, kind = cpu_oracle()
     threads = os.cpu_count() or 1
-    rate, done = o.time_roundtrip(f, i, sample_input(4096), threads, seconds)
+    sample = sample_input(4096)
+    rate, done = o.time_roundtrip(f, i, sample, threads, seconds)
+    one = max(1.0, seconds / 2)
+    rate1, done1 = o.time_roundtrip(f, i, sample, 1, one)
     return {"value": rate, "unit": "polys/s", "cores": threads, "kind": kind,
             "sample": f"NTT+iNTT round trips over a 4096-polynomial sample per thread, "
-                      f"repeated for {seconds:.0f} s on {threads} threads ({done} polys)"}
+                      f"repeated for {seconds:.0f} s on {threads} threads ({done} polys)",
+            "one_core": {"value": rate1, "unit": "polys/s", "cores": 1,
+                         "sample": f"the same on one thread for {one:.0f} s ({done1} polys)"}}
+
+
+def reference_gpu(npoly: int, runs: int = 30):
+    """The reference's own GPU benchmark (ntt_bench/ntt_bench.cu:909-991, its
+    kernels built unmodified for sm_100a into oracle/_ref/ntt_bench), run on
+    this GPU at the same batch size; its summary table is parsed (median
+    polys/s of NTT, iNTT and the round trip, per variant; the reference times
+    every launch with its own events, ntt_bench/ntt_bench.cu:637-661)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ntt_bench")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ntt_bench not built (make -C oracle gpubar)"}
+    try:
+        p = subprocess.run([exe, str(npoly), str(runs)], capture_output=True, text=True,
+                           timeout=300)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "ntt_bench did not finish in 300 s"}
+    rows = {}
+    in_table = False
+    for line in p.stdout.splitlines():
+        if line.startswith(" SUMMARY"):
+            in_table = True
+            continue
+        if not in_table or "|" not in line or line.startswith("Variant") or line.startswith("-"):
+            continue
+        parts = [x.strip() for x in line.split("|")]
+        try:
+            nums = [float(v) for v in parts[1].split() + parts[2].split() + parts[3].split()]
+        except (ValueError, IndexError):
+            continue
+        name = parts[0][:30].strip()   # %-30s variant label, then geometry and block
+        ok = parts[4].split() if len(parts) > 4 else []
+        rows[name] = {"ntt_med_polys_s": nums[1] * 1e6, "intt_med_polys_s": nums[3] * 1e6,
+                      "roundtrip_med_polys_s": nums[5] * 1e6,
+                      "parity_ok": ok == ["ok", "ok"]}
+    if p.returncode != 0 or not rows:
+        return {"unavailable": f"ntt_bench exited {p.returncode} ({len(rows)} rows parsed)",
+                "stdout_tail": p.stdout[-400:]}
+    best = max(rows, key=lambda k: rows[k]["roundtrip_med_polys_s"])
+    return {"value": rows[best]["roundtrip_med_polys_s"], "unit": "polys/s",
+            "best_variant": best, "npoly": npoly, "runs": runs, "variants": rows,
+            "how": "oracle/_ref/ntt_bench <npoly> <runs>: the reference's kernels built for "
+                   "sm_100a, run on this GPU; median round trip of its best variant"}
 
 
 def run_reference(args):
@@ -189,8 +253,11 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "polys/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
+        "scaling": "strong", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
         "config": config(args.npoly, world),
+        "cpu_processes": 1,
+        "note": "one CPU process on rank 0's host at every --gpus: the reference's C "
+                "ntt()/invntt() has no GPU path, so its value does not grow with N",
         "cpu_baseline": {"value": value, "unit": "polys/s", "cores": threads, "kind": kind,
                          "sample": "each step: NTT then iNTT on a 4096-polynomial sample "
                                    f"of the workload, split over {threads} threads"},
@@ -234,24 +301,29 @@ def run_ours(args):
     torch.cuda.synchronize()
 
     K = args.steps
-    # timed region: K steps back to back (no events between the launches, so
-    # consecutive kernels overlap prologue and tail through programmatic launch)
+    R = max(1, args.repeats)
+    # timed regions: R regions of exactly K steps back to back (no events
+    # between the launches, so consecutive kernels overlap prologue and tail
+    # through programmatic launch), each bracketed by a barrier and a
+    # synchronize; the value is the median region (max over ranks per region)
     e_start = torch.cuda.Event(enable_timing=True)
     e_end = torch.cuda.Event(enable_timing=True)
     sampler = ClockSampler(local)
     sampler.start()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e_start.record(stream)
-    for k in range(K):
-        step(k)
-    e_end.record(stream)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    region_ms = []
+    for _ in range(R):
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e_start.record(stream)
+        for k in range(K):
+            step(k)
+        e_end.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        region_ms.append(e_start.elapsed_time(e_end))
     clocks = sampler.stop()
-    total_ms = e_start.elapsed_time(e_end)
     # per-launch split (batch latency p50/p99): the same workload with an event
     # around each launch, which serialises the launches
     K2 = min(K, 2000)
@@ -279,7 +351,8 @@ def run_ours(args):
         g1.record(stream)
         torch.cuda.synchronize()
         group_ms[name] = g0.elapsed_time(g1) / K2
-    total_ms = tkdist.max_over_ranks(total_ms, dist, device="cuda")
+    region_ms = [tkdist.max_over_ranks(t, dist, device="cuda") for t in region_ms]
+    total_ms = statistics.median(region_ms)
     status = tk.device_status(local)
     if status:
         raise RuntimeError(f"kernel status flags {status:#x}")
@@ -336,11 +409,20 @@ def run_ours(args):
                            "batch_roundtrip_p99": 1e3 * lat_rt[min(K2 - 1, int(0.99 * K2))]},
             "e2e": e2e,
             "gpu_launches": 2 * K,
+            "repeats": {"regions": R, "steps_per_region": K,
+                        "ms_per_step_min": min(region_ms) / K,
+                        "ms_per_step_median": total_ms / K,
+                        "ms_per_step_max": max(region_ms) / K,
+                        "how": "value and ms_per_step from the median of R timed regions of "
+                               "K steps each (gpu_launches counts one region)"},
             "kernel_split_steps": K2,
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        if world == 1 and not args.no_reference_gpu:
+            torch.cuda.synchronize()
+            line["reference_gpu"] = reference_gpu(n)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -715,8 +797,35 @@ def run_serve(args):
     }), flush=True)
 
 
+def free_port() -> int:
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def launch_ranks(args) -> int:
+    """--gpus N without a launcher: start N ranks (one per GPU) with
+    torch.distributed.run on this node and return its exit status."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1",
+           f"--master-port={free_port()}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
+    world_env = os.environ.get("WORLD_SIZE")
+    single = args.serve or args.forms or args.matvec or args.sweep
+    if args.gpus < 1:
+        sys.exit("bench.py: --gpus must be at least 1")
+    if single and (args.gpus > 1 or (world_env is not None and int(world_env) > 1)):
+        sys.exit("bench.py: --serve, --forms, --matvec and --sweep run on one GPU (--gpus 1)")
+    if world_env is None and args.gpus > 1:
+        sys.exit(launch_ranks(args))
+    if world_env is not None and int(world_env) != args.gpus:
+        sys.exit(f"bench.py: launched with WORLD_SIZE={world_env} but --gpus {args.gpus}; "
+                 "pass --gpus equal to the number of ranks")
     if args.serve:
         run_serve(args)
     elif args.forms:

@@ -663,11 +663,17 @@ static __device__ __align__(256) uint8_t g_noalloc_scratch[TK_NOALLOC_SCRATCH_BY
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_ptr[kMaxDevices];
 
+constexpr int kNoallocMaxBatches = 16;
+
 int tk_matvec_host_noalloc(const tk_matvec_batch* batches, int nbatches, tk_stream_t stream) {
   t_err[0] = 0;
   int nonempty = 0;
   int rc = validate_matvec(batches, nbatches, true, &nonempty);
   if (rc || nonempty == 0) return rc;
+  if (nbatches > kNoallocMaxBatches) {  // before any device work
+    set_msg("tk_matvec_host_noalloc: at most 16 batches per call");
+    return TK_ERR_INVALID_VALUE;
+  }
   size_t need = 0;
   for (int b = 0; b < nbatches; b++) {
     const tk_matvec_batch& B = batches[b];
@@ -700,11 +706,7 @@ int tk_matvec_host_noalloc(const tk_matvec_batch* batches, int nbatches, tk_stre
     scratch = (uint8_t*)g_noalloc_ptr[dev];
   }
   cudaStream_t st = (cudaStream_t)stream;
-  tk_matvec_batch dev_batches[16];
-  if (nbatches > 16) {
-    set_msg("tk_matvec_host_noalloc: at most 16 batches per call");
-    return TK_ERR_INVALID_VALUE;
-  }
+  tk_matvec_batch dev_batches[kNoallocMaxBatches] = {};
   cudaError_t e = cudaSuccess;
   size_t off = 0;
   for (int b = 0; b < nbatches && e == cudaSuccess; b++) {

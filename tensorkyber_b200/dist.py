@@ -5,8 +5,9 @@ independent, so N processes (one per GPU) each transform a contiguous range
 of the batch and there is no exchange step on the data path.  This module
 holds the host-side pieces: reading the launcher's environment, the
 contiguous shard of each rank, the max-over-ranks timing reduction, and
-gathering shards back to one rank.  They run on any torch.distributed
-backend (NCCL between GPUs, gloo on the CPU for tests).
+gathering shards back to one rank.  They run on NCCL between GPUs (the
+buffers they exchange then live on the rank's current CUDA device) and on
+gloo on the CPU (tests).
 """
 from __future__ import annotations
 
@@ -54,12 +55,17 @@ def max_over_ranks(value: float, dist=None, device=None) -> float:
     return float(t.item())
 
 
-def gather_shards(local: np.ndarray, n: int, dist=None, dst: int = 0):
+def gather_shards(local: np.ndarray, n: int, dist=None, dst: int = 0, device=None):
     """Concatenates every rank's shard (rank order) on rank `dst`; returns the
-    full (n, ...) array there and None elsewhere.  Shards follow shard()."""
+    full (n, ...) array there and None elsewhere.  Shards follow shard().
+    Point-to-point buffers go on `device`: by default the current CUDA device
+    under NCCL (which moves only CUDA tensors) and host memory otherwise."""
     if dist is None:
         return local
     import torch
+    if device is None:
+        device = (torch.device("cuda", torch.cuda.current_device())
+                  if dist.get_backend() == "nccl" else torch.device("cpu"))
     rank, world = dist.get_rank(), dist.get_world_size()
     start, stop = shard(n, rank, world)
     if local.shape[0] != stop - start:
@@ -72,9 +78,10 @@ def gather_shards(local: np.ndarray, n: int, dist=None, dst: int = 0):
             if r == dst:
                 continue
             a, b = shard(n, r, world)
-            buf = torch.empty((b - a,) + tail, dtype=torch.from_numpy(local[:0]).dtype)
+            buf = torch.empty((b - a,) + tail, dtype=torch.from_numpy(local[:0]).dtype,
+                              device=device)
             dist.recv(buf, src=r)
-            out[a:b] = buf.numpy()
+            out[a:b] = buf.cpu().numpy()
         return out
-    dist.send(torch.from_numpy(np.ascontiguousarray(local)), dst=dst)
+    dist.send(torch.from_numpy(np.ascontiguousarray(local)).to(device), dst=dst)
     return None

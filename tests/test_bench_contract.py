@@ -65,3 +65,34 @@ def test_default_arguments():
     finally:
         sys.argv = argv
     assert a.gpus == 1 and a.impl == "ours" and a.warmup >= 3
+
+
+def test_gpus_without_a_launcher_starts_the_ranks_itself():
+    """--gpus 2 run directly (no torchrun) starts two ranks through
+    torch.distributed.run instead of silently running one process; rank 0
+    prints the only line, with n_gpus = 2."""
+    import signal
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+           "--steps", "2", "--warmup", "1"]
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT")}
+    p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True,
+                         cwd=ROOT, env=env, start_new_session=True)
+    try:
+        out, err = p.communicate(timeout=300)
+    except subprocess.TimeoutExpired:
+        os.killpg(p.pid, signal.SIGKILL)
+        raise
+    assert p.returncode == 0, err[-2000:]
+    lines = [l for l in out.splitlines() if l.strip().startswith("{")]
+    assert len(lines) == 1, out
+    d = json.loads(lines[0])
+    assert d["n_gpus"] == 2 and d["cpu_processes"] == 1 and d["value"] > 0
+
+
+def test_gpus_must_match_the_launched_ranks():
+    env = dict(os.environ, WORLD_SIZE="2", RANK="0", LOCAL_RANK="0")
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "1",
+                        "--steps", "1", "--warmup", "3"],
+                       capture_output=True, text=True, timeout=120, cwd=ROOT, env=env)
+    assert p.returncode != 0 and "WORLD_SIZE=2" in p.stderr

@@ -244,3 +244,52 @@ def test_matvec_mixed_k_in_place_many_batches(tk, cuda, oracle, mode):
     for (k, A, s, e), out in zip(items, outs):
         assert (canon(out) == canon(oracle_out(oracle, k, A, s, e))).all()
     assert tk.device_status(0) == 0
+
+
+def test_matvec_graph_replay_matches_oracle(tk, cuda, oracle, mode):
+    """tk_matvec captured in a CUDA graph (three mixed-k batches, the form the
+    matrix-vector benchmark replays), replayed twice with new inputs written
+    into the captured buffers in between: each replay equals the oracle's
+    composition of the reference's ntt / basemul / invntt."""
+    torch = cuda
+    tk.init(0)
+    spec = ((2, 70), (3, 41), (4, 29))
+    dev = []
+    for k, n in spec:
+        dev.append((k, torch.empty((n, k, k, 256), dtype=torch.int16, device="cuda"),
+                    torch.empty((n, k, 256), dtype=torch.int16, device="cuda"),
+                    torch.empty((n, k, 256), dtype=torch.int16, device="cuda"),
+                    torch.empty((n, k, 256), dtype=torch.int16, device="cuda")))
+
+    def fill(seed):
+        host = []
+        for i, ((k, n), (_, tA, ts, te, _o)) in enumerate(zip(spec, dev)):
+            A, s, e = make_jobs(seed + i, k, n)
+            tA.copy_(torch.from_numpy(A))
+            ts.copy_(torch.from_numpy(s))
+            te.copy_(torch.from_numpy(e))
+            host.append((k, A, s, e))
+        torch.cuda.synchronize()
+        return host
+
+    fill(500)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        tk.matvec(dev, stream=side)               # warm-up outside the capture
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        tk.matvec(dev)
+    for rep, seed in enumerate((600, 700)):
+        host = fill(seed)
+        for d in dev:
+            d[4].fill_(0x2B2B)
+        torch.cuda.synchronize()
+        graph.replay()
+        torch.cuda.synchronize()
+        for (k, A, s, e), d in zip(host, dev):
+            out = d[4].cpu().numpy()
+            assert (canon(out) == canon(oracle_out(oracle, k, A, s, e))).all(), (rep, k)
+    del graph
+    assert tk.device_status(0) == 0

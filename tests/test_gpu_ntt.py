@@ -253,6 +253,43 @@ def test_large_batch_every_coefficient(tk, cuda, oracle):
     assert tk.device_status(0) == 0
 
 
+HEADLINE = 262144
+
+
+def test_headline_configuration_every_coefficient(tk, cuda, oracle):
+    """The configuration the headline metric is quoted on: 262,144
+    polynomials, uniform in [0, q), forward and inverse as separate launches
+    with the variants the library picks for that size.  Every coefficient of
+    both directions is compared with the oracle (the inverse on the raw input,
+    not only through the round trip)."""
+    n = HEADLINE
+    x = rng(262144).integers(0, Q, size=(n, 256), dtype=np.int16)
+    t = to_dev(cuda, x)
+    tk.ntt(t)
+    cuda.cuda.synchronize()
+    check_fwd(t.cpu().numpy(), oracle.ntt(x))
+    t = to_dev(cuda, x)
+    tk.invntt(t)
+    cuda.cuda.synchronize()
+    check_inv(t.cpu().numpy(), oracle.invntt(x))
+    assert tk.device_status(0) == 0
+
+
+@pytest.mark.parametrize("variant", range(NVARIANTS))
+def test_headline_size_every_inverse_variant(tk, cuda, oracle, variant):
+    """Each inverse variant at the headline size, every coefficient against
+    the oracle, inputs over the full int16 range."""
+    n = HEADLINE
+    x = rng(4000 + variant).integers(-32768, 32768, size=(n, 256), dtype=np.int16)
+    try:
+        tk.set_variant(tk.INVERSE, variant)
+        out = gpu_inv(tk, cuda, x)
+    finally:
+        tk.set_variant(tk.INVERSE, -1)
+    check_inv(out, oracle.invntt(canon(x).astype(np.int16)))
+    assert tk.device_status(0) == 0
+
+
 def test_reference_name_shims(tk, cuda, oracle):
     """libtk_pqcrystals.so exports the reference's own symbol names
     (ntt_bench/ref/ntt.h under KYBER_NAMESPACE) and matches the oracle mod q."""
