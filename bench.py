@@ -61,7 +61,11 @@ def parse():
                    help="skip the reference's own GPU kernels (oracle/_ref/ntt_bench)")
     p.add_argument("--cpu-seconds", type=float, default=6.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--variant", type=int, default=-1, help="force a kernel variant (-1: auto)")
+    p.add_argument("--variant", type=int, default=-1,
+                   help="force a kernel variant in both directions (-1: auto; 4 is inverse only "
+                        "and then forces only the inverse)")
+    p.add_argument("--fwd-variant", type=int, default=-1, help="force the forward's variant")
+    p.add_argument("--inv-variant", type=int, default=-1, help="force the inverse's variant")
     p.add_argument("--sweep", action="store_true",
                    help="batch-size sweep 2^0..2^sweep-max (autotuned), JSON lines to --sweep-out")
     p.add_argument("--sweep-max", type=int, default=24)
@@ -270,6 +274,15 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------- ours ---
+def apply_variants(tk, args):
+    fwd = args.fwd_variant if args.fwd_variant >= 0 else args.variant
+    inv = args.inv_variant if args.inv_variant >= 0 else args.variant
+    if fwd >= 0 and fwd != 4:
+        tk.set_variant(tk.FORWARD, fwd)
+    if inv >= 0:
+        tk.set_variant(tk.INVERSE, inv)
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -283,9 +296,7 @@ def run_ours(args):
     # one process per GPU; NCCL only carries the barrier and the timing max
     dist = tkdist.init("nccl", 120.0, device=torch.device("cuda", local))
     tk.init(local)
-    if args.variant >= 0:
-        tk.set_variant(tk.FORWARD, args.variant)
-        tk.set_variant(tk.INVERSE, args.variant)
+    apply_variants(tk, args)
     n = args.npoly
     gen = np.random.default_rng(1000 + rank)
     batches = [torch.from_numpy(gen.integers(0, Q, size=(n, 256), dtype=np.int16)).cuda()

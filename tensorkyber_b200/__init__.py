@@ -172,7 +172,8 @@ def get_table(which: int) -> np.ndarray:
     """Host matrix builder output (no GPU needed): 0 M1, 1 M2, 2 MA, 3 Minv as
     int16 residues; 4 / 5 the forward / inverse fragment tables as raw uint32;
     6 the basemul pair constants as int32[128]; 7 the tiled matrix-vector
-    kernel's inverse fragment tables (2^-16 * invntt) as raw uint32."""
+    kernel's inverse fragment tables (2^-16 * invntt) as raw uint32; 8 the
+    tcgen05 inverse's 36 int8 B-operand tiles of 1 KiB, raw (view as uint8)."""
     L = lib()
     size = L.tk_get_table(which, None, 0)
     if size < 0:

@@ -56,6 +56,7 @@ const char* const kVariantNames[tk::kNumMmaVariants] = {
     "mma.sync 8 warps x 64-poly tiles, 3-slot TMA ring",
     "mma.sync 4 warps x 32-poly tiles, 2-slot TMA ring",
     "mma.sync 4 warps x 32-poly tiles, 2-slot TMA ring, int32 stage-1 tile",
+    "tcgen05 kind::i8, 128-poly tiles, TMEM accumulators and stage-B operand (inverse only)",
 };
 
 // Autotuned choice per direction and size bucket floor(log2(npoly)); -1 =
@@ -145,7 +146,8 @@ int ensure_ready(int dev, DeviceInfo** out) {
     S.info.cc_major = p.major;
     S.info.cc_minor = p.minor;
     S.info.total_mem = p.totalGlobalMem;
-    if (!tk::mma_init_device(&S.info) || !tk::matvec_init_device()) {
+    if (!tk::mma_init_device(&S.info) || !tk::matvec_init_device() ||
+        !tk::tc5_init_device(&S.info)) {
       set_err("kernel set-up", cudaGetLastError());
       return TK_ERR_CUDA;
     }
@@ -844,9 +846,9 @@ const char* tk_variant_name(int variant) {
 
 int tk_set_variant(int direction, int variant) {
   t_err[0] = 0;
-  if ((direction != TK_FORWARD && direction != TK_INVERSE) || variant < -1 ||
-      variant >= tk::kNumMmaVariants) {
-    set_msg("tk_set_variant: bad direction or variant");
+  if ((direction != TK_FORWARD && direction != TK_INVERSE) ||
+      (variant != -1 && !tk::variant_valid(direction == TK_INVERSE, variant))) {
+    set_msg("tk_set_variant: bad direction or variant (variant 4 is inverse only)");
     return TK_ERR_INVALID_VALUE;
   }
   g_forced[direction == TK_INVERSE ? 1 : 0].store(variant);
@@ -902,8 +904,8 @@ static int load_tuning(const char* path) {
     double us;
     int n = 0;
     while (fscanf(f, "%d %d %d %lf", &dir, &bucket, &variant, &us) == 4) {
-      if (dir < 0 || dir > 1 || bucket < 0 || bucket >= kBuckets || variant < 0 ||
-          variant >= tk::kNumMmaVariants) {
+      if (dir < 0 || dir > 1 || bucket < 0 || bucket >= kBuckets ||
+          !tk::variant_valid(dir == 1, variant)) {
         n = -1;
         break;
       }
@@ -950,6 +952,7 @@ int tk_autotune(int device, size_t max_npoly, const char* cache_path) {
       best_us[dir][b] = 1e30;
       best_v[dir][b] = 0;
       for (int v = 0; v < tk::kNumMmaVariants && e == cudaSuccess; v++) {
+        if (!tk::variant_valid(dir == 1, v)) continue;
         for (int w = 0; w < 2 && e == cudaSuccess; w++)
           e = tk::launch_mma(dir == 1, v, buf, buf, (long long)n, *info, st);
         if (e == cudaSuccess) e = cudaEventRecord(e0, st);
@@ -1003,6 +1006,7 @@ long long tk_get_table(int which, void* out, size_t bytes) {
   static tk::FwdFrags FF;
   static tk::InvFrags IF, IFR;
   static int32_t ZR[128];
+  static uint8_t TC5[tk::kTc5TableBytes];
   static std::once_flag once;
   std::call_once(once, [] {
     tk::build_matrices(&M);
@@ -1012,6 +1016,7 @@ long long tk_get_table(int which, void* out, size_t bytes) {
     tk::Matrices MR = M;
     tk::scale_inverse(&MR, 169);  // 2^-16 mod q
     tk::build_inv_frags(MR, &IFR);
+    tk::build_tc5_tables(M, TC5);
   });
   const void* src;
   size_t size;
@@ -1024,6 +1029,7 @@ long long tk_get_table(int which, void* out, size_t bytes) {
     case 5: src = &IF; size = sizeof(IF); break;
     case 6: src = ZR; size = sizeof(ZR); break;
     case 7: src = &IFR; size = sizeof(IFR); break;
+    case 8: src = TC5; size = sizeof(TC5); break;
     default: return -TK_ERR_INVALID_VALUE;
   }
   if (out) memcpy(out, src, bytes < size ? bytes : size);

@@ -6,13 +6,21 @@
 
 namespace tk {
 
-// mma.sync kernel variants (CTA shape / pipeline depth):
+// Kernel variants.  mma.sync (CTA shape / pipeline depth):
 //   0: 4 warps, 32-polynomial tiles, 3 slots   (4 CTAs/SM)
 //   1: 8 warps, 64-polynomial tiles, 3 slots   (2 CTAs/SM)
 //   2: 4 warps, 32-polynomial tiles, 2 slots   (6 CTAs/SM)
 //   3: 4 warps, 32-polynomial tiles, 2 slots, forward stage 1 kept as int32
 //      sums in a shared-memory tile (3 CTAs/SM)
-constexpr int kNumMmaVariants = 4;
+// tcgen05 (inverse only):
+//   4: 128-polynomial tiles, tcgen05.mma kind::i8 with tensor-memory
+//      accumulators, stage B's operand in tensor memory (tk_tc5.cu; 1 CTA/SM)
+constexpr int kNumMmaSyncVariants = 4;
+constexpr int kTc5Variant = 4;
+constexpr int kNumMmaVariants = 5;
+inline bool variant_valid(bool inverse, int v) {
+  return v >= 0 && v < kNumMmaVariants && (inverse || v != kTc5Variant);
+}
 // Largest batch one kernel launch covers (TMA coordinates are signed 32-bit).
 constexpr long long kMaxLaunchPolys = 1ll << 30;
 
@@ -24,12 +32,13 @@ struct DeviceInfo {
   int device = -1;
   int num_sms = 0;
   int cc_major = 0, cc_minor = 0;
-  int mma_ctas_per_sm[2][kNumMmaVariants] = {{1, 1, 1, 1}, {1, 1, 1, 1}};  // [inverse][variant]
+  int mma_ctas_per_sm[2][kNumMmaSyncVariants] = {{1, 1, 1, 1}, {1, 1, 1, 1}};  // [inverse][variant]
   int form_ctas_per_sm[kNumInputForms] = {1, 1, 1};  // forward input forms 1..3
-  int add_ctas_per_sm[kNumMmaVariants] = {1, 1, 1, 1};  // inverse with addend
+  int add_ctas_per_sm[kNumMmaSyncVariants] = {1, 1, 1, 1};  // inverse with addend
   int multi_ctas_per_sm[3] = {1, 1, 1};  // multi-segment forward / inverse / inverse+addend
   int tile_ctas_per_sm = 1;              // k_matvec_tiles
   size_t total_mem = 0;
+  unsigned* status = nullptr;            // the device's kernel status flags (device address)
 };
 
 // Uploads the constant fragment tables to the current device and fills the
@@ -63,8 +72,16 @@ cudaError_t launch_mma_segs(bool inverse, int variant, const Seg* segs, int nseg
                             const DeviceInfo& info, cudaStream_t stream);
 
 // CUresult of the calling thread's last tensor-map encode (launch_mma reports
-// cudaErrorInvalidResourceHandle when an encode failed).
+// cudaErrorInvalidResourceHandle when an encode failed); note_encode_result
+// records one from another unit.
 int last_encode_result();
+void note_encode_result(int r);
+
+// The tcgen05 inverse (tk_tc5.cu): per-device set-up (constant tiles, shared
+// memory limit) and the batched inverse src -> dst (src == dst in place).
+bool tc5_init_device(DeviceInfo* info);
+cudaError_t launch_invntt_tc5(const int16_t* src, int16_t* dst, long long npoly,
+                              const DeviceInfo& info, cudaStream_t stream);
 
 // Matrix-vector jobs (tk_matvec.cu).  Chunks hold at most this many vector
 // polynomials, so that intermediates stay in the 126 MB L2.

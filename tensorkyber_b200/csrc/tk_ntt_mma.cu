@@ -967,8 +967,8 @@ constexpr Variant make_variant() {
                  C::kTile};
 }
 
-// [inverse][variant]
-static const Variant kVariants[2][kNumMmaVariants] = {
+// [inverse][variant] (the mma.sync variants; variant 4 is tk_tc5.cu's)
+static const Variant kVariants[2][kNumMmaSyncVariants] = {
     {make_variant<false, 4, 3>(), make_variant<false, 8, 3>(), make_variant<false, 4, 2>(),
      make_variant<false, 4, 2, kInInt16, false, OneSeg, true>()},
     {make_variant<true, 4, 3>(), make_variant<true, 8, 3>(), make_variant<true, 4, 2>(),
@@ -976,7 +976,7 @@ static const Variant kVariants[2][kNumMmaVariants] = {
 };
 // Inverse with an addend (the matrix-vector pipeline's iNTT + e), per variant;
 // the plain inverse does not carry the addend's loads and adds.
-static const Variant kAddVariants[kNumMmaVariants] = {
+static const Variant kAddVariants[kNumMmaSyncVariants] = {
     make_variant<true, 4, 3, kInInt16, true>(), make_variant<true, 8, 3, kInInt16, true>(),
     make_variant<true, 4, 2, kInInt16, true>(),
     make_variant<true, 4, 2, kInInt16, true, OneSeg, true>()};
@@ -1051,6 +1051,7 @@ static bool encode_packed_map(CUtensorMap* map, const void* base, int npoly, int
 }
 
 int last_encode_result() { return g_last_encode_result; }
+void note_encode_result(int r) { g_last_encode_result = r; }
 
 static bool upload_tables_current_device() {
   static Matrices M, MR;
@@ -1077,8 +1078,11 @@ static bool upload_tables_current_device() {
 
 bool mma_init_device(DeviceInfo* info) {
   if (!upload_tables_current_device()) return false;
+  void* st = nullptr;
+  if (cudaGetSymbolAddress(&st, g_status) != cudaSuccess || !st) return false;
+  info->status = (unsigned*)st;
   for (int inv = 0; inv < 2; inv++)
-    for (int v = 0; v < kNumMmaVariants; v++) {
+    for (int v = 0; v < kNumMmaSyncVariants; v++) {
       const Variant& V = kVariants[inv][v];
       if (cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, V.smem) !=
           cudaSuccess)
@@ -1089,7 +1093,7 @@ bool mma_init_device(DeviceInfo* info) {
         return false;
       info->mma_ctas_per_sm[inv][v] = per_sm > 0 ? per_sm : 1;
     }
-  for (int v = 0; v < kNumMmaVariants; v++) {
+  for (int v = 0; v < kNumMmaSyncVariants; v++) {
     const Variant& V = kAddVariants[v];
     if (cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, V.smem) !=
         cudaSuccess)
@@ -1189,9 +1193,22 @@ struct Piece {
 
 cudaError_t launch_mma_segs(bool inverse, int variant, const Seg* segs, int nseg,
                             const DeviceInfo& info, cudaStream_t stream) {
-  if (variant < 0 || variant >= kNumMmaVariants) variant = 0;
+  if (!variant_valid(inverse, variant)) variant = 0;
   bool add_form = false;
   for (int j = 0; j < nseg; j++) add_form |= inverse && segs[j].addend != nullptr;
+  // the tcgen05 inverse: plain inverse batches, one at a time; the addend form
+  // (and several batches in one launch) run the mma.sync shapes
+  if (variant == kTc5Variant) {
+    if (!add_form) {
+      for (int j = 0; j < nseg; j++) {
+        const cudaError_t e =
+            launch_invntt_tc5(segs[j].src, segs[j].dst, segs[j].npoly, info, stream);
+        if (e != cudaSuccess) return e;
+      }
+      return cudaSuccess;
+    }
+    variant = 0;
+  }
   // pieces of at most kMaxLaunchPolys, in order
   Piece pc[kMaxSegs];
   int np = 0;

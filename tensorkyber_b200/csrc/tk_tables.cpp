@@ -255,4 +255,27 @@ void build_inv_frags(const Matrices& M, InvFrags* F) {
     }
 }
 
+void build_tc5_tables(const Matrices& M, uint8_t* out) {
+  memset(out, 0, kTc5TableBytes);
+  auto put = [&](int tile, int n, int k, int64_t v) {
+    out[tile * kTc5TileBytes + tc5_tile_offset(n, k)] = (uint8_t)v;
+  };
+  for (int m = 0; m < 16; m++)
+    for (int o = 0; o < 16; o++)
+      for (int g = 0; g < 2; g++)
+        for (int ci = 0; ci < 16; ci++) {
+          put(2 * m, o + 16 * g, 2 * ci, limb(M.ma[m][o][ci], g));
+          put(2 * m + 1, o + 16 * g, 2 * ci + 1, limb(byte_weighted(M.ma[m][o][ci], 1), g));
+        }
+  for (int h = 0; h < 2; h++)
+    for (int i = 0; i < 16; i++)
+      for (int g = 0; g < 2; g++)
+        for (int mm = 0; mm < 8; mm++) {
+          const int m = 8 * h + mm;
+          for (int j = 0; j < 3; j++)
+            put(32 + 2 * h, i + 16 * g, 4 * mm + j, limb(byte_weighted(M.minv[i][m], j), g));
+          put(32 + 2 * h + 1, i + 16 * g, 4 * mm + 3, limb(byte_weighted(M.minv[i][m], 3), g));
+        }
+}
+
 }  // namespace tk

@@ -122,6 +122,30 @@ void build_pair_roots(int32_t z[128]);
 // built from M compute f * invntt.
 void scale_inverse(Matrices* M, int64_t f);
 
+// B operands of the TMEM inverse (tk_tc5.cu), one 1 KiB tile per MMA shape:
+// N = 32 rows (n = out + 16 * limb: output coefficient, 7-bit limb of the
+// constant) x K = 32 bytes, int8 values, in the tcgen05 K-major layout
+// without swizzle: row n, K byte k at (n / 8) * 256 + (k / 16) * 128 +
+// (n % 8) * 16 + k % 16 (8-row core matrices of 16 bytes per row; the two
+// K halves 128 bytes apart, 8-row groups 256 bytes apart).
+//   tile 2m + t      stage A (MA of block m): K byte k = 2 c' + b, byte b of
+//                    input coefficient c'.  t = 0 (unsigned data): the low
+//                    bytes, constant MA[m][out][c']; t = 1 (signed data): the
+//                    high bytes, constant 256 MA[m][out][c'] mod q; the other
+//                    byte's rows are zero.
+//   tile 32 + 2h + t stage B (Minv), K step h: K byte k = 4 (m - 8h) + j,
+//                    byte j of the int32 stage-A sum of block m.  t = 0
+//                    (unsigned): bytes 0-2, constant Minv[out][m] 256^j mod
+//                    q; t = 1 (signed): byte 3, constant Minv[out][m] 2^24
+//                    mod q; the other bytes' rows are zero.
+constexpr int kTc5TileBytes = 1024;
+constexpr int kTc5Tiles = 36;
+constexpr int kTc5TableBytes = kTc5Tiles * kTc5TileBytes;
+inline int tc5_tile_offset(int n, int k) {
+  return (n >> 3) * 256 + (k >> 4) * 128 + (n & 7) * 16 + (k & 15);
+}
+void build_tc5_tables(const Matrices& M, uint8_t* out /* kTc5TableBytes */);
+
 void build_matrices(Matrices* M);
 void build_fwd_frags(const Matrices& M, FwdFrags* F);
 void build_inv_frags(const Matrices& M, InvFrags* F);

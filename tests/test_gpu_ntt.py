@@ -57,15 +57,22 @@ def test_uniform_sizes(tk, cuda, oracle, n):
     check_inv(gpu_inv(tk, cuda, x), oracle.invntt(x))
 
 
-NVARIANTS = 4
+NVARIANTS = 5
+TC5 = 4          # the tcgen05 inverse: inverse only
+
+
+def force_variant(tk, variant):
+    """Both directions to `variant` (the inverse only for the tcgen05 one)."""
+    if variant != TC5:
+        tk.set_variant(tk.FORWARD, variant)
+    tk.set_variant(tk.INVERSE, variant)
 
 
 @pytest.mark.parametrize("variant", range(NVARIANTS))
 def test_every_variant(tk, cuda, oracle, variant):
     assert tk.variant_count() == NVARIANTS
     try:
-        tk.set_variant(tk.FORWARD, variant)
-        tk.set_variant(tk.INVERSE, variant)
+        force_variant(tk, variant)
         for n in (1, 9, 63, 64, 65, 1000, 20001):
             x = rng(100 + n).integers(-4000, 4000, size=(n, 256)).astype(np.int16)
             check_fwd(gpu_fwd(tk, cuda, x), oracle.ntt(x))
@@ -337,8 +344,7 @@ def test_every_variant_many_tiles_per_cta(tk, cuda, oracle, variant):
     x = rng(5150).integers(-32768, 32768, size=(n, 256)).astype(np.int16)
     base_f, base_i = gpu_fwd(tk, cuda, x), gpu_inv(tk, cuda, x)
     try:
-        tk.set_variant(tk.FORWARD, variant)
-        tk.set_variant(tk.INVERSE, variant)
+        force_variant(tk, variant)
         f, i = gpu_fwd(tk, cuda, x), gpu_inv(tk, cuda, x)
     finally:
         tk.set_variant(tk.FORWARD, -1)
@@ -392,3 +398,37 @@ def test_sweep_maximum_size_properties(tk, cuda):
                        (fa.to(torch.int64) + fb.to(torch.int64)) % Q)
     torch.cuda.synchronize()
     assert tk.device_status(0) == 0
+
+
+def test_tcgen05_inverse_tile_boundaries_and_guards(tk, cuda, oracle):
+    """The tcgen05 inverse's 128-polynomial tiles: sizes on and around tile and
+    grid boundaries (one tile per SM and more), out of place with guard
+    polynomials around the output that must stay untouched, every coefficient
+    against the oracle and byte-equal to the mma.sync inverse."""
+    torch = cuda
+    try:
+        for n in (1, 127, 128, 129, 255, 256, 148 * 128 - 1, 148 * 128 + 1, 3 * 148 * 128 + 77):
+            x = rng(9000 + n).integers(-32768, 32768, size=(n, 256), dtype=np.int16)
+            base = gpu_inv(tk, cuda, x)
+            tk.set_variant(tk.INVERSE, TC5)
+            src = to_dev(torch, x)
+            guard = 3
+            out = torch.full(((n + 2 * guard), 256), 0x7E7E, dtype=torch.int16, device="cuda")
+            tk.invntt(src, out=out[guard:guard + n])
+            torch.cuda.synchronize()
+            o = out.cpu().numpy()
+            assert (o[:guard] == 0x7E7E).all() and (o[guard + n:] == 0x7E7E).all(), n
+            assert (src.cpu().numpy() == x).all(), n            # input untouched
+            got = o[guard:guard + n]
+            tk.set_variant(tk.INVERSE, -1)
+            assert (got == base).all(), n
+            pick = np.unique(np.r_[0:min(n, 300), max(0, n - 300):n])
+            check_inv(got[pick], oracle.invntt(canon(x[pick]).astype(np.int16)))
+    finally:
+        tk.set_variant(tk.INVERSE, -1)
+    assert tk.device_status(0) == 0
+
+
+def test_tcgen05_forward_variant_is_rejected(tk):
+    with pytest.raises(tk.TKError):
+        tk.set_variant(tk.FORWARD, TC5)
