@@ -56,7 +56,7 @@ const char* const kVariantNames[tk::kNumMmaVariants] = {
     "mma.sync 8 warps x 64-poly tiles, 3-slot TMA ring",
     "mma.sync 4 warps x 32-poly tiles, 2-slot TMA ring",
     "mma.sync 4 warps x 32-poly tiles, 2-slot TMA ring, int32 stage-1 tile",
-    "tcgen05 kind::i8, 128-poly tiles, TMEM accumulators and stage-B operand (inverse only)",
+    "tcgen05 kind::i8, 128-poly tiles, TMEM accumulators and second-stage operand",
 };
 
 // Autotuned choice per direction and size bucket floor(log2(npoly)); -1 =
@@ -848,7 +848,7 @@ int tk_set_variant(int direction, int variant) {
   t_err[0] = 0;
   if ((direction != TK_FORWARD && direction != TK_INVERSE) ||
       (variant != -1 && !tk::variant_valid(direction == TK_INVERSE, variant))) {
-    set_msg("tk_set_variant: bad direction or variant (variant 4 is inverse only)");
+    set_msg("tk_set_variant: bad direction or variant");
     return TK_ERR_INVALID_VALUE;
   }
   g_forced[direction == TK_INVERSE ? 1 : 0].store(variant);

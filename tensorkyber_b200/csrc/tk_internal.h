@@ -12,15 +12,14 @@ namespace tk {
 //   2: 4 warps, 32-polynomial tiles, 2 slots   (6 CTAs/SM)
 //   3: 4 warps, 32-polynomial tiles, 2 slots, forward stage 1 kept as int32
 //      sums in a shared-memory tile (3 CTAs/SM)
-// tcgen05 (inverse only):
+// tcgen05:
 //   4: 128-polynomial tiles, tcgen05.mma kind::i8 with tensor-memory
-//      accumulators, stage B's operand in tensor memory (tk_tc5.cu; 1 CTA/SM)
+//      accumulators, the second stage's operand in tensor memory (tk_tc5.cu;
+//      1 CTA/SM)
 constexpr int kNumMmaSyncVariants = 4;
 constexpr int kTc5Variant = 4;
 constexpr int kNumMmaVariants = 5;
-inline bool variant_valid(bool inverse, int v) {
-  return v >= 0 && v < kNumMmaVariants && (inverse || v != kTc5Variant);
-}
+inline bool variant_valid(bool /*inverse*/, int v) { return v >= 0 && v < kNumMmaVariants; }
 // Largest batch one kernel launch covers (TMA coordinates are signed 32-bit).
 constexpr long long kMaxLaunchPolys = 1ll << 30;
 
@@ -77,11 +76,11 @@ cudaError_t launch_mma_segs(bool inverse, int variant, const Seg* segs, int nseg
 int last_encode_result();
 void note_encode_result(int r);
 
-// The tcgen05 inverse (tk_tc5.cu): per-device set-up (constant tiles, shared
-// memory limit) and the batched inverse src -> dst (src == dst in place).
+// The tcgen05 kernels (tk_tc5.cu): per-device set-up (constant tiles, shared
+// memory limits) and the batched transform src -> dst (src == dst in place).
 bool tc5_init_device(DeviceInfo* info);
-cudaError_t launch_invntt_tc5(const int16_t* src, int16_t* dst, long long npoly,
-                              const DeviceInfo& info, cudaStream_t stream);
+cudaError_t launch_tc5(bool inverse, const int16_t* src, int16_t* dst, long long npoly,
+                       const DeviceInfo& info, cudaStream_t stream);
 
 // Matrix-vector jobs (tk_matvec.cu).  Chunks hold at most this many vector
 // polynomials, so that intermediates stay in the 126 MB L2.

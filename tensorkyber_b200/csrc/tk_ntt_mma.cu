@@ -1196,13 +1196,13 @@ cudaError_t launch_mma_segs(bool inverse, int variant, const Seg* segs, int nseg
   if (!variant_valid(inverse, variant)) variant = 0;
   bool add_form = false;
   for (int j = 0; j < nseg; j++) add_form |= inverse && segs[j].addend != nullptr;
-  // the tcgen05 inverse: plain inverse batches, one at a time; the addend form
-  // (and several batches in one launch) run the mma.sync shapes
+  // the tcgen05 kernels: plain batches, one launch each; the inverse with an
+  // addend runs the mma.sync shapes
   if (variant == kTc5Variant) {
     if (!add_form) {
       for (int j = 0; j < nseg; j++) {
-        const cudaError_t e =
-            launch_invntt_tc5(segs[j].src, segs[j].dst, segs[j].npoly, info, stream);
+        const cudaError_t e = launch_tc5(inverse, segs[j].src, segs[j].dst, segs[j].npoly, info,
+                                         stream);
         if (e != cudaSuccess) return e;
       }
       return cudaSuccess;

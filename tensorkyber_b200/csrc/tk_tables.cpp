@@ -276,6 +276,24 @@ void build_tc5_tables(const Matrices& M, uint8_t* out) {
             put(32 + 2 * h, i + 16 * g, 4 * mm + j, limb(byte_weighted(M.minv[i][m], j), g));
           put(32 + 2 * h + 1, i + 16 * g, 4 * mm + 3, limb(byte_weighted(M.minv[i][m], 3), g));
         }
+  for (int i = 0; i < 16; i++)
+    for (int g = 0; g < 2; g++)
+      for (int m = 0; m < 16; m++) {
+        put(36, i + 16 * g, 2 * m, limb(M.m1[i][m], g));
+        put(37, i + 16 * g, 2 * m + 1, limb(byte_weighted(M.m1[i][m], 1), g));
+      }
+  for (int i = 0; i < 16; i++)
+    for (int h = 0; h < 2; h++)
+      for (int o = 0; o < 16; o++)
+        for (int g = 0; g < 2; g++)
+          for (int cc = 0; cc < 8; cc++) {
+            const int c = 8 * h + cc;
+            for (int j = 0; j < 3; j++)
+              put(38 + 4 * i + 2 * h, o + 16 * g, 4 * cc + j,
+                  limb(byte_weighted(M.m2[i][o][c], j), g));
+            put(38 + 4 * i + 2 * h + 1, o + 16 * g, 4 * cc + 3,
+                limb(byte_weighted(M.m2[i][o][c], 3), g));
+          }
 }
 
 }  // namespace tk

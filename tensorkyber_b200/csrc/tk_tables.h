@@ -138,8 +138,18 @@ void scale_inverse(Matrices* M, int64_t f);
 //                    (unsigned): bytes 0-2, constant Minv[out][m] 256^j mod
 //                    q; t = 1 (signed): byte 3, constant Minv[out][m] 2^24
 //                    mod q; the other bytes' rows are zero.
+//   tile 36 + t      forward stage 1 (M1): K byte k = 2 m + b, byte b of the
+//                    block-m coefficient; t = 0: low bytes, constant
+//                    M1[out][m]; t = 1: high bytes, 256 M1[out][m] mod q.
+//   tile 38 + 4i + 2h + t  forward stage 2 (M2 of block i), K step h: K byte
+//                    k = 4 (c - 8h) + j, byte j of the int32 stage-1 sum of
+//                    coefficient c; t = 0: bytes 0-2, constant M2[i][out][c]
+//                    256^j mod q; t = 1: byte 3, M2[i][out][c] 2^24 mod q.
+// The inverse uses tiles 0-35, the forward tiles 36-101.
 constexpr int kTc5TileBytes = 1024;
-constexpr int kTc5Tiles = 36;
+constexpr int kTc5InvTiles = 36;
+constexpr int kTc5FwdTiles = 66;
+constexpr int kTc5Tiles = kTc5InvTiles + kTc5FwdTiles;
 constexpr int kTc5TableBytes = kTc5Tiles * kTc5TileBytes;
 inline int tc5_tile_offset(int n, int k) {
   return (n >> 3) * 256 + (k >> 4) * 128 + (n & 7) * 16 + (k & 15);

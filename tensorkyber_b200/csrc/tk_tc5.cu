@@ -64,16 +64,23 @@ constexpr int kTcSlotBytes = 4 * kTcQuarterBytes;  // 64 KiB
 constexpr int kTcEpiWarps = 8;
 constexpr int kTcMmaWarp = 8, kTcTmaWarp = 9;
 constexpr int kTcThreads = 32 * (kTcEpiWarps + 2);
-// dynamic shared memory, from a 1024-byte aligned base (the swizzle atom)
+// dynamic shared memory, from a 1024-byte aligned base (the swizzle atom):
+// two 64 KiB tile slots, this direction's constant tiles, the mbarriers
+// (in_full[2], out_ready[2], d_full[2], d_empty[2], y_full, x_ready, consts,
+// drain, x_read) and the tensor-memory base address
 constexpr int kOffTables = 2 * kTcSlotBytes;
-constexpr int kOffBars = kOffTables + kTc5TableBytes;
-// in_full[2], out_ready[2], d_full[2], d_empty[2], y_full, consts, drain
-constexpr int kNumBars = 11;
-constexpr int kOffTmemSlot = kOffBars + 8 * kNumBars;
-constexpr int kTcSmemUsed = kOffTmemSlot + 8;
-constexpr int kTcSmemBytes = kTcSmemUsed + 1024;  // + slack to align the base
-static_assert(2 * kTcSmemBytes > 228 * 1024, "one CTA per SM: it owns all tensor memory");
-static_assert(kTcSmemBytes <= 227 * 1024, "shared memory per CTA");
+constexpr int kNumBars = 13;
+template <bool kInverse>
+struct Tc5Layout {
+  static constexpr int kTiles = kInverse ? kTc5InvTiles : kTc5FwdTiles;
+  static constexpr int kFirstTile = kInverse ? 0 : kTc5InvTiles;
+  static constexpr int kTableBytes = kTiles * kTc5TileBytes;
+  static constexpr int kOffBars = kOffTables + kTableBytes;
+  static constexpr int kOffTmemSlot = kOffBars + 8 * kNumBars;
+  static constexpr int kSmemBytes = kOffTmemSlot + 8 + 1024;  // + slack to align the base
+  static_assert(2 * kSmemBytes > 228 * 1024, "one CTA per SM: it owns all tensor memory");
+  static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
+};
 // tensor memory
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kColY = 0;
@@ -84,9 +91,10 @@ constexpr uint32_t kColD0 = 256;  // accumulator buffer b at kColD0 + 128 b
 constexpr uint32_t kIdescU8 = (2u << 4) | (4u << 17) | (8u << 24);
 constexpr uint32_t kIdescS8 = kIdescU8 | (1u << 7) | (1u << 10);
 constexpr uint64_t kWaitNs = 2000000000ull;
-// centred reduction of stage B's sums (red_centred_wide below)
+// exact reductions of the second stage's sums (red_*_wide below)
 constexpr int64_t kM40 = 330282857;  // ceil(2^40 / q) = floor(2^40 / q) + 1
-constexpr int64_t kAdd40 = (3329ll * 65536 + 1664) * kM40;
+constexpr int64_t kAddCentred40 = (3329ll * 65536 + 1664) * kM40;
+constexpr int64_t kAddExact40 = (3329ll * 65536) * kM40;
 
 __device__ __align__(128) uint8_t g_tc5_tables[kTc5TableBytes];
 
@@ -105,7 +113,13 @@ constexpr uint32_t kLayoutNone = 0, kLayoutSw128 = 2;
 // exactly there (the multiplier's error adds < 2^28 / 2^40 < 1/q), as one
 // 64-bit multiply-add; S - q quot differs from T - q quot by q 2^16.
 __device__ __forceinline__ uint32_t red_centred_wide(uint32_t s) {
-  const int64_t x = (int64_t)(int32_t)s * kM40 + kAdd40;
+  const int64_t x = (int64_t)(int32_t)s * kM40 + kAddCentred40;
+  const uint32_t quot = (uint32_t)((uint64_t)x >> 40);
+  return s - quot * 3329u;
+}
+// The same for the canonical residue in [0, q): floor(T / q).
+__device__ __forceinline__ uint32_t red_exact_wide(uint32_t s) {
+  const int64_t x = (int64_t)(int32_t)s * kM40 + kAddExact40;
   const uint32_t quot = (uint32_t)((uint64_t)x >> 40);
   return s - quot * 3329u;
 }
@@ -113,16 +127,56 @@ __device__ __forceinline__ uint32_t red_centred_wide(uint32_t s) {
 __device__ __forceinline__ void st_shared_v2(uint32_t addr, uint32_t a, uint32_t b) {
   asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(addr), "r"(a), "r"(b) : "memory");
 }
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c,
+                                             uint32_t d) {
+  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c),
+               "r"(d)
+               : "memory");
+}
+__device__ __forceinline__ uint4 ld_shared_v4(uint32_t addr) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(addr)
+               : "memory");
+  return v;
+}
 
 struct Tc5Params {
   CUtensorMap in;   // [npoly][256] uint16, boxes 64 x 128 rows, 128-byte swizzle
   CUtensorMap out;  // the same for the output (equal to in for in place)
-  const uint8_t* tables;
+  const uint8_t* tables;  // this direction's constant tiles (device copy)
   unsigned* status;
   int ntiles;
 };
 
-__global__ void __launch_bounds__(kTcThreads, 1) k_invntt_tc5(const __grid_constant__ Tc5Params P) {
+// Address of row p's 16-byte chunk k (0..31: bytes 16k .. 16k+15 of the
+// natural 512-byte row) in a slot holding the TMA layout: quarter k / 8,
+// rows 128 bytes apart, chunk index xor (p % 8) (the 128-byte swizzle).
+__device__ __forceinline__ uint32_t sw128_chunk(uint32_t slot, uint32_t p, uint32_t k) {
+  return slot + (k >> 3) * kTcQuarterBytes + p * 128u + (((k & 7u) ^ (p & 7u)) << 4);
+}
+
+// kInverse: see the file comment.  Forward (the same roles and pipeline):
+//   * the 8 epilogue warps first transpose the loaded tile in place into
+//     stage 1's A operand: for coefficient c (c-tile c, 4 KiB at 4096 c of
+//     the slot), row p's 32 K bytes are the blocks' values X[m][c] in block
+//     order (K byte 2m + b), K-major without swizzle (8-row core matrices of
+//     16-byte rows, the two K halves 128 bytes apart, 8-row groups 256 bytes
+//     apart); warp w reads coefficients 8 (w / 4) .. + 7 of every block of its
+//     rows, a CTA-wide barrier of those warps, then every warp writes its
+//     c-tiles;
+//   * stage 1 (M1 over m): per c-tile one unsigned and one signed MMA from
+//     shared memory, chunks of c-tiles {0-3}, {4-7}, {8-11}, {12-15}; its
+//     sums go to tensor memory as column 16 i + c (block i, coefficient c);
+//   * stage 2 (M2^(i) of block i): four MMAs per block from tensor-memory
+//     columns 16 i .. 16 i + 15 (bytes 0-2 unsigned, byte 3 signed) against
+//     the block's own constant tiles, chunks of blocks {0-3}, {4-7}, ...;
+//     exact reduction to [0, q), natural-order rows written to the slot in
+//     the TMA layout (two 16-byte chunks per block).
+template <bool kInverse>
+__global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ Tc5Params P) {
+  using L = Tc5Layout<kInverse>;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -134,12 +188,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_invntt_tc5(const __grid_const
   const int nmine = t_end - t_begin;
 
   const uint32_t tables = base + kOffTables;
-  const uint32_t bars = base + kOffBars;
+  const uint32_t bars = base + L::kOffBars;
   auto in_full = [&](int s) { return bars + 8u * s; };
   auto out_ready = [&](int s) { return bars + 16u + 8u * s; };
   auto d_full = [&](int b) { return bars + 32u + 8u * b; };
   auto d_empty = [&](int b) { return bars + 48u + 8u * b; };
-  const uint32_t y_full = bars + 64u, consts = bars + 72u, drain = bars + 80u;
+  const uint32_t y_full = bars + 64u, x_ready = bars + 72u, consts = bars + 80u,
+                 drain = bars + 88u, x_read = bars + 96u;
   auto slot_addr = [&](int s) { return base + (uint32_t)s * kTcSlotBytes; };
 
   if (tid == 0) {
@@ -150,22 +205,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_invntt_tc5(const __grid_const
       mbar_init(d_empty(s), 4);
     }
     mbar_init(y_full, kTcEpiWarps);
+    mbar_init(x_ready, kTcEpiWarps);
     mbar_init(consts, 1);
     mbar_init(drain, 1);
+    mbar_init(x_read, kTcEpiWarps);
     fence_mbar_init();
   }
   if (warp == kTcMmaWarp) {
-    tmem_alloc(base + kOffTmemSlot, kTmemCols);
+    tmem_alloc(base + L::kOffTmemSlot, kTmemCols);
     tmem_relinquish();
   }
   if (warp == kTcTmaWarp && lane == 0) {  // constant tiles (written once by the host)
-    mbar_expect_tx(consts, kTc5TableBytes);
-    bulk_g2s(tables, P.tables, kTc5TableBytes, consts);
+    mbar_expect_tx(consts, L::kTableBytes);
+    bulk_g2s(tables, P.tables, L::kTableBytes, consts);
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = *(volatile uint32_t*)(basep + kOffTmemSlot);
+  const uint32_t tmem = *(volatile uint32_t*)(basep + L::kOffTmemSlot);
   // the tile data may have been written by the previous kernel in the stream
   grid_dependency_wait();
   grid_launch_dependents();
@@ -207,7 +264,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_invntt_tc5(const __grid_const
     if (lane == 0 && nmine > 0) {
       // ---- MMA issuer ----
       auto tile_desc = [&](int i) {
-        return smem_desc(tables + (uint32_t)i * kTc5TileBytes, 128, 256, kLayoutNone);
+        return smem_desc(tables + (uint32_t)(i - L::kFirstTile) * kTc5TileBytes, 128, 256,
+                         kLayoutNone);
       };
       uint32_t use[2] = {0, 0};
       auto take = [&](int b) {  // the buffer's previous contents were read out
@@ -219,40 +277,56 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_invntt_tc5(const __grid_const
       ok = mbar_wait_bounded(consts, 0, kWaitNs);
       for (int k = 0; k < nmine && ok; k++) {
         const int s = k & 1;
-        if (!(ok = mbar_wait_bounded(in_full(s), (uint32_t)(k >> 1) & 1u, kWaitNs))) break;
+        // inverse: the loaded tile is stage A's operand; forward: wait for
+        // the epilogue warps' transposed copy of it
+        if (kInverse)
+          ok = mbar_wait_bounded(in_full(s), (uint32_t)(k >> 1) & 1u, kWaitNs);
+        else
+          ok = mbar_wait_bounded(x_ready, (uint32_t)k & 1u, kWaitNs);
+        if (!ok) break;
         tc_fence_after();
-        // stage A: chunk j = blocks 4j .. 4j+3 (input quarter j)
+        // first stage: chunk j = four MMA pairs (inverse: blocks 4j..4j+3 of
+        // input quarter j; forward: c-tiles 4j..4j+3)
         for (int j = 0; j < 4 && ok; j++) {
           const int b = j & 1;
           if (!(ok = take(b))) break;
 #pragma unroll
-          for (int mm = 0; mm < 4; mm++) {
-            const int m = 4 * j + mm;
-            const uint64_t a =
-                smem_desc(slot_addr(s) + j * kTcQuarterBytes + 32 * mm, 16, 1024, kLayoutSw128);
-            const uint32_t d = tmem + (kColD0 + 128u * b) + 32u * mm;
-            tc_mma_ss(d, a, tile_desc(2 * m), kIdescU8, 0);
-            tc_mma_ss(d, a, tile_desc(2 * m + 1), kIdescS8, 1);
+          for (int u = 0; u < 4; u++) {
+            const int idx = 4 * j + u;
+            const uint32_t d = tmem + kColD0 + 128u * b + 32u * u;
+            if (kInverse) {
+              const uint64_t a = smem_desc(slot_addr(s) + j * kTcQuarterBytes + 32 * u, 16, 1024,
+                                           kLayoutSw128);
+              tc_mma_ss(d, a, tile_desc(2 * idx), kIdescU8, 0);
+              tc_mma_ss(d, a, tile_desc(2 * idx + 1), kIdescS8, 1);
+            } else {
+              const uint64_t a = smem_desc(slot_addr(s) + 4096u * idx, 128, 256, kLayoutNone);
+              tc_mma_ss(d, a, tile_desc(36), kIdescU8, 0);
+              tc_mma_ss(d, a, tile_desc(37), kIdescS8, 1);
+            }
           }
           tc_commit(d_full(b));
           use[b]++;
         }
         if (!ok) break;
-        // stage B: coefficient sets {0-3}, {8-11}, {4-7}, {12-15}
+        // second stage from tensor memory: inverse coefficient sets {0-3},
+        // {8-11}, {4-7}, {12-15}; forward blocks {0-3}, {4-7}, ...
         if (!(ok = mbar_wait_bounded(y_full, (uint32_t)k & 1u, kWaitNs))) break;
         tc_fence_after();
         for (int j = 0; j < 4 && ok; j++) {
           const int b = j & 1;
           if (!(ok = take(b))) break;
-          const int c0 = 8 * (j & 1) + 4 * (j >> 1);
+          const int first = kInverse ? 8 * (j & 1) + 4 * (j >> 1) : 4 * j;
 #pragma unroll
           for (int u = 0; u < 4; u++) {
-            const uint32_t d = tmem + (kColD0 + 128u * b) + 32u * u;
+            const int idx = first + u;
+            const uint32_t d = tmem + kColD0 + 128u * b + 32u * u;
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-              const uint32_t a = tmem + kColY + 16u * (c0 + u) + 8u * h;
-              tc_mma_ts(d, a, tile_desc(32 + 2 * h), kIdescU8, h);
-              tc_mma_ts(d, a, tile_desc(33 + 2 * h), kIdescS8, 1);
+              const uint32_t a = tmem + kColY + 16u * idx + 8u * h;
+              const int tl = kInverse ? 32 + 2 * h : 38 + 4 * idx + 2 * h;
+              tc_mma_ts(d, a, tile_desc(tl), kIdescU8, h);
+              tc_mma_ts(d, a, tile_desc(tl + 1), kIdescS8, 1);
             }
           }
           tc_commit(d_full(b));
@@ -267,7 +341,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_invntt_tc5(const __grid_const
     // ---- warps 0-7: tensor memory <-> registers <-> shared memory ----
     const int half = warp >> 2, lq = warp & 3;
     const uint32_t lanes = (uint32_t)(32 * lq) << 16;
-    const uint32_t dcol = tmem + lanes + (kColD0 + 128u * half);
+    const uint32_t dcol = tmem + lanes + kColD0 + 128u * half;
     const uint32_t ycol = tmem + lanes + kColY;
     const uint32_t p = (uint32_t)(32 * lq + lane);  // polynomial (row) of the tile
     uint32_t use = 0;
@@ -284,7 +358,42 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_invntt_tc5(const __grid_const
     };
     for (int k = 0; k < nmine && ok; k++) {
       const int s = k & 1;
-      // stage A chunks j = half, half + 2: S[m][c] -> column 16 c + m
+      const uint32_t slot = slot_addr(s);
+      if (!kInverse) {
+        // transpose the loaded tile in place into stage 1's operand
+        const bool landed = mbar_wait_bounded(in_full(s), (uint32_t)(k >> 1) & 1u, kWaitNs);
+        uint4 R[16];  // X[m][8 half .. 8 half + 7] as four coefficient pairs
+#pragma unroll
+        for (int m = 0; m < 16; m++) R[m] = ld_shared_v4(sw128_chunk(slot, p, 2u * m + half));
+        // every warp's rows read before any c-tile is written over them
+        __syncwarp();
+        if (lane == 0) mbar_arrive(x_read);
+        const bool read = mbar_wait_bounded(x_read, (uint32_t)k & 1u, kWaitNs);
+        if (!__all_sync(0xffffffffu, landed && read)) {
+          ok = false;
+          break;
+        }
+#pragma unroll
+        for (int cc = 0; cc < 8; cc++) {
+          const uint32_t sel = (cc & 1) ? 0x7632u : 0x5410u;
+          uint32_t w[8];
+#pragma unroll
+          for (int mp = 0; mp < 8; mp++) {
+            const uint4 a = R[2 * mp], b = R[2 * mp + 1];
+            const uint32_t wa = (cc >> 1) == 0 ? a.x : (cc >> 1) == 1 ? a.y : (cc >> 1) == 2 ? a.z : a.w;
+            const uint32_t wb = (cc >> 1) == 0 ? b.x : (cc >> 1) == 1 ? b.y : (cc >> 1) == 2 ? b.z : b.w;
+            w[mp] = __byte_perm(wa, wb, sel);
+          }
+          const uint32_t xa = slot + 4096u * (8u * half + cc) + (p >> 3) * 256u + (p & 7u) * 16u;
+          st_shared_v4(xa, w[0], w[1], w[2], w[3]);
+          st_shared_v4(xa + 128u, w[4], w[5], w[6], w[7]);
+        }
+        fence_proxy_async_smem();  // generic-proxy writes -> the tensor cores
+        __syncwarp();
+        if (lane == 0) mbar_arrive(x_ready);
+      }
+      // first stage's sums -> tensor memory column 16 n + idx (n: the MMA's
+      // output column, idx: its position in the chunk), chunks j = half, half + 2
 #pragma unroll 1
       for (int jj = 0; jj < 2; jj++) {
         const int j = half + 2 * jj;
@@ -298,21 +407,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_invntt_tc5(const __grid_const
         tc_wait_ld();
         give_back();
 #pragma unroll
-        for (int c = 0; c < 16; c++)
-          tc_st4(ycol + 16u * c + 4u * j, r0[c] + (r0[16 + c] << 7), r0[32 + c] + (r0[48 + c] << 7),
-                 r1[c] + (r1[16 + c] << 7), r1[32 + c] + (r1[48 + c] << 7));
+        for (int n = 0; n < 16; n++)
+          tc_st4(ycol + 16u * n + 4u * j, r0[n] + (r0[16 + n] << 7), r0[32 + n] + (r0[48 + n] << 7),
+                 r1[n] + (r1[16 + n] << 7), r1[32 + n] + (r1[48 + n] << 7));
       }
       if (!ok) break;
       tc_wait_st();
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(y_full);
-      // stage B chunks: coefficients c0 .. c0+3 of every block i
-      const uint32_t slot = slot_addr(s);
+      // second stage: reduce, pack, write the output rows into the slot
 #pragma unroll 1
       for (int jj = 0; jj < 2; jj++) {
         const int j = half + 2 * jj;
-        const int c0 = 8 * (j & 1) + 4 * (j >> 1);
         if (!__all_sync(0xffffffffu, take())) {
           ok = false;
           break;
@@ -322,18 +429,34 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_invntt_tc5(const __grid_const
         tc_ld64(dcol + 64, r1);
         tc_wait_ld();
         give_back();
-        // row p, coefficients 16 i + c0 .. +3: 8 bytes at byte 32 (i % 4) +
-        // 2 c0 of quarter i / 4, 16-byte chunk index xor (p % 8) (the swizzle)
+        if (kInverse) {
+          // coefficients 16 i + c0 .. +3 of every block i: 8 bytes at byte
+          // 2 c0 % 16 of 16-byte chunk 2 i + c0 / 8
+          const int c0 = 8 * (j & 1) + 4 * (j >> 1);
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
-          const uint32_t z0 = red_centred_wide(r0[i] + (r0[16 + i] << 7));
-          const uint32_t z1 = red_centred_wide(r0[32 + i] + (r0[48 + i] << 7));
-          const uint32_t z2 = red_centred_wide(r1[i] + (r1[16 + i] << 7));
-          const uint32_t z3 = red_centred_wide(r1[32 + i] + (r1[48 + i] << 7));
-          const uint32_t chunk = 2u * (i & 3) + (uint32_t)(c0 >> 3);
-          const uint32_t addr = slot + (uint32_t)(i >> 2) * kTcQuarterBytes + p * 128u +
-                                ((chunk ^ (p & 7u)) << 4) + 8u * ((uint32_t)(c0 >> 2) & 1u);
-          st_shared_v2(addr, pack2(z0, z1), pack2(z2, z3));
+          for (int i = 0; i < 16; i++) {
+            const uint32_t z0 = red_centred_wide(r0[i] + (r0[16 + i] << 7));
+            const uint32_t z1 = red_centred_wide(r0[32 + i] + (r0[48 + i] << 7));
+            const uint32_t z2 = red_centred_wide(r1[i] + (r1[16 + i] << 7));
+            const uint32_t z3 = red_centred_wide(r1[32 + i] + (r1[48 + i] << 7));
+            st_shared_v2(sw128_chunk(slot, p, 2u * i + (uint32_t)(c0 >> 3)) +
+                             8u * ((uint32_t)(c0 >> 2) & 1u),
+                         pack2(z0, z1), pack2(z2, z3));
+          }
+        } else {
+          // blocks 4j .. 4j+3, each 16 coefficients = two 16-byte chunks
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const uint32_t* r = u < 2 ? r0 + 32 * u : r1 + 32 * (u - 2);
+            uint32_t w[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++)
+              w[t] = pack2(red_exact_wide(r[2 * t] + (r[16 + 2 * t] << 7)),
+                           red_exact_wide(r[2 * t + 1] + (r[17 + 2 * t] << 7)));
+            const uint32_t i = 4u * j + u;
+            st_shared_v4(sw128_chunk(slot, p, 2u * i), w[0], w[1], w[2], w[3]);
+            st_shared_v4(sw128_chunk(slot, p, 2u * i + 1), w[4], w[5], w[6], w[7]);
+          }
         }
       }
       if (!ok) break;
@@ -349,7 +472,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_invntt_tc5(const __grid_const
     tc_fence_after();
     tmem_dealloc(tmem, kTmemCols);
   }
-  if (!ok) atomicOr(P.status, 2u);
+  if (!ok) atomicOr(P.status, kInverse ? 2u : 1u);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encoder() {
@@ -402,15 +525,20 @@ bool tc5_init_device(DeviceInfo* info) {
   void* p = nullptr;
   if (cudaGetSymbolAddress(&p, g_tc5_tables) != cudaSuccess || !p) return false;
   g_tables_ptr[info->device] = (const uint8_t*)p;
-  return cudaFuncSetAttribute((const void*)k_invntt_tc5,
+  return cudaFuncSetAttribute((const void*)k_tc5<true>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              kTcSmemBytes) == cudaSuccess;
+                              Tc5Layout<true>::kSmemBytes) == cudaSuccess &&
+         cudaFuncSetAttribute((const void*)k_tc5<false>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              Tc5Layout<false>::kSmemBytes) == cudaSuccess;
 }
 
-cudaError_t launch_invntt_tc5(const int16_t* src, int16_t* dst, long long npoly,
-                              const DeviceInfo& info, cudaStream_t stream) {
+cudaError_t launch_tc5(bool inverse, const int16_t* src, int16_t* dst, long long npoly,
+                       const DeviceInfo& info, cudaStream_t stream) {
   const uint8_t* tables = g_tables_ptr[info.device];
   if (!tables || !info.status) return cudaErrorInitializationError;
+  const void* fn = inverse ? (const void*)k_tc5<true> : (const void*)k_tc5<false>;
+  const int smem = inverse ? Tc5Layout<true>::kSmemBytes : Tc5Layout<false>::kSmemBytes;
   for (long long done = 0; done < npoly; done += kMaxLaunchPolys) {
     const int n = (int)((npoly - done) < kMaxLaunchPolys ? (npoly - done) : kMaxLaunchPolys);
     Tc5Params m = {};
@@ -419,14 +547,14 @@ cudaError_t launch_invntt_tc5(const int16_t* src, int16_t* dst, long long npoly,
       m.out = m.in;
     else if (!encode_swizzled_map(&m.out, dst + done * 256, n))
       return cudaErrorInvalidResourceHandle;
-    m.tables = tables;
+    m.tables = tables + (inverse ? 0 : kTc5InvTiles * kTc5TileBytes);
     m.status = info.status;
     m.ntiles = (n + kTcTile - 1) / kTcTile;
     const int ctas = m.ntiles < info.num_sms ? m.ntiles : info.num_sms;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)ctas);
     cfg.blockDim = dim3((unsigned)kTcThreads);
-    cfg.dynamicSmemBytes = (size_t)kTcSmemBytes;
+    cfg.dynamicSmemBytes = (size_t)smem;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -434,7 +562,7 @@ cudaError_t launch_invntt_tc5(const int16_t* src, int16_t* dst, long long npoly,
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     void* args[1] = {(void*)&m};
-    const cudaError_t e = cudaLaunchKernelExC(&cfg, (const void*)k_invntt_tc5, args);
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

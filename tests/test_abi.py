@@ -81,10 +81,11 @@ def test_variant_selection(tk):
     assert 0 <= tk.get_variant(tk.FORWARD, 1000) < tk.variant_count()
     assert L.tk_get_variant(7, 10) < 0
     assert tk.variant_count() == 5
-    assert L.tk_set_variant(tk.FORWARD, 4) == 1          # tcgen05 variant: inverse only
-    assert L.tk_set_variant(tk.INVERSE, 4) == 0
-    assert tk.get_variant(tk.INVERSE, 1000) == 4
-    tk.set_variant(tk.INVERSE, -1)
+    assert L.tk_set_variant(tk.FORWARD, 5) == 1
+    for d in (tk.FORWARD, tk.INVERSE):                   # the tcgen05 variant
+        assert L.tk_set_variant(d, 4) == 0
+        assert tk.get_variant(d, 1000) == 4
+        tk.set_variant(d, -1)
     assert "tcgen05" in tk.variant_name(4)
 
 
@@ -94,7 +95,7 @@ def test_get_table_sizes(tk):
     assert L.tk_get_table(1, None, 0) == 16 * 16 * 16 * 2
     assert L.tk_get_table(6, None, 0) == 128 * 4
     assert L.tk_get_table(7, None, 0) == L.tk_get_table(5, None, 0)
-    assert L.tk_get_table(8, None, 0) == 36 * 1024            # the tcgen05 inverse's tiles
+    assert L.tk_get_table(8, None, 0) == 102 * 1024           # the tcgen05 kernels' tiles
     assert L.tk_get_table(9, None, 0) < 0
     assert L.tk_get_table(-1, None, 0) < 0
     small = (ctypes.c_uint8 * 4)()

@@ -200,7 +200,7 @@ def test_matvec_full_mixed_workload_sample(tk, cuda, oracle, mode):
     assert tk.device_status(0) == 0
 
 
-@pytest.mark.parametrize("variant", range(4))
+@pytest.mark.parametrize("variant", range(5))
 def test_matvec_pipeline_every_variant(tk, cuda, oracle, variant):
     """The pipeline's forward and inverse-with-addend launches in each batch
     kernel variant (one batch, so the single-batch kernels run)."""

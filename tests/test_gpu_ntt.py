@@ -58,13 +58,11 @@ def test_uniform_sizes(tk, cuda, oracle, n):
 
 
 NVARIANTS = 5
-TC5 = 4          # the tcgen05 inverse: inverse only
+TC5 = 4          # the tcgen05 kernels
 
 
 def force_variant(tk, variant):
-    """Both directions to `variant` (the inverse only for the tcgen05 one)."""
-    if variant != TC5:
-        tk.set_variant(tk.FORWARD, variant)
+    tk.set_variant(tk.FORWARD, variant)
     tk.set_variant(tk.INVERSE, variant)
 
 
@@ -400,35 +398,53 @@ def test_sweep_maximum_size_properties(tk, cuda):
     assert tk.device_status(0) == 0
 
 
-def test_tcgen05_inverse_tile_boundaries_and_guards(tk, cuda, oracle):
-    """The tcgen05 inverse's 128-polynomial tiles: sizes on and around tile and
+@pytest.mark.parametrize("inverse", [False, True], ids=["forward", "inverse"])
+def test_tcgen05_tile_boundaries_and_guards(tk, cuda, oracle, inverse):
+    """The tcgen05 kernels' 128-polynomial tiles: sizes on and around tile and
     grid boundaries (one tile per SM and more), out of place with guard
-    polynomials around the output that must stay untouched, every coefficient
-    against the oracle and byte-equal to the mma.sync inverse."""
+    polynomials around the output that must stay untouched, in place too,
+    every coefficient against the oracle and byte-equal to the mma.sync
+    kernels."""
     torch = cuda
+    d = tk.INVERSE if inverse else tk.FORWARD
+    run = gpu_inv if inverse else gpu_fwd
+    ref = oracle.invntt if inverse else oracle.ntt
+    check = check_inv if inverse else check_fwd
+    fn = tk.invntt if inverse else tk.ntt
     try:
         for n in (1, 127, 128, 129, 255, 256, 148 * 128 - 1, 148 * 128 + 1, 3 * 148 * 128 + 77):
             x = rng(9000 + n).integers(-32768, 32768, size=(n, 256), dtype=np.int16)
-            base = gpu_inv(tk, cuda, x)
-            tk.set_variant(tk.INVERSE, TC5)
+            tk.set_variant(d, 0)
+            base = run(tk, cuda, x)
+            tk.set_variant(d, TC5)
             src = to_dev(torch, x)
             guard = 3
             out = torch.full(((n + 2 * guard), 256), 0x7E7E, dtype=torch.int16, device="cuda")
-            tk.invntt(src, out=out[guard:guard + n])
+            fn(src, out=out[guard:guard + n])
             torch.cuda.synchronize()
             o = out.cpu().numpy()
             assert (o[:guard] == 0x7E7E).all() and (o[guard + n:] == 0x7E7E).all(), n
             assert (src.cpu().numpy() == x).all(), n            # input untouched
             got = o[guard:guard + n]
-            tk.set_variant(tk.INVERSE, -1)
             assert (got == base).all(), n
+            assert (run(tk, cuda, x) == base).all(), n          # in place
             pick = np.unique(np.r_[0:min(n, 300), max(0, n - 300):n])
-            check_inv(got[pick], oracle.invntt(canon(x[pick]).astype(np.int16)))
+            check(got[pick], ref(canon(x[pick]).astype(np.int16)))
     finally:
-        tk.set_variant(tk.INVERSE, -1)
+        tk.set_variant(d, -1)
     assert tk.device_status(0) == 0
 
 
-def test_tcgen05_forward_variant_is_rejected(tk):
-    with pytest.raises(tk.TKError):
-        tk.set_variant(tk.FORWARD, TC5)
+@pytest.mark.parametrize("variant", range(NVARIANTS))
+def test_headline_size_every_forward_variant(tk, cuda, oracle, variant):
+    """Each forward variant at the headline size, every coefficient against
+    the oracle, inputs over the full int16 range."""
+    n = HEADLINE
+    x = rng(5000 + variant).integers(-32768, 32768, size=(n, 256), dtype=np.int16)
+    try:
+        tk.set_variant(tk.FORWARD, variant)
+        out = gpu_fwd(tk, cuda, x)
+    finally:
+        tk.set_variant(tk.FORWARD, -1)
+    check_fwd(out, oracle.ntt(canon(x).astype(np.int16)))
+    assert tk.device_status(0) == 0

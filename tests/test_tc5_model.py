@@ -1,4 +1,4 @@
-"""CPU model of the tcgen05 inverse (tensorkyber_b200/csrc/tk_tc5.cu).
+"""CPU model of the tcgen05 kernels (tensorkyber_b200/csrc/tk_tc5.cu).
 
 The library's own B-operand tiles (table 8) are decoded from the tcgen05
 K-major layout and pushed through the kernel's integer steps with numpy: stage
@@ -24,15 +24,18 @@ def tile_offset(n, k):
     return (n >> 3) * 256 + (k >> 4) * 128 + (n & 7) * 16 + (k & 15)
 
 
+NTILES = 102          # 0-35 the inverse's, 36-101 the forward's
+
+
 def decode(raw: np.ndarray) -> np.ndarray:
-    """36 tiles of B[n][k] (n = out + 16 limb, k = K byte), each read back from
+    """The tiles of B[n][k] (n = out + 16 limb, k = K byte), each read back from
     the K-major core-matrix layout; even tiles as unsigned, odd as signed."""
     raw = raw.view(np.uint8)
-    assert raw.size == 36 * TILE_BYTES
+    assert raw.size == NTILES * TILE_BYTES
     off = np.array([[tile_offset(n, k) for k in range(32)] for n in range(32)])
     assert sorted(off.ravel().tolist()) == list(range(TILE_BYTES))   # a bijection
-    tiles = np.zeros((36, 32, 32), dtype=np.int64)
-    for t in range(36):
+    tiles = np.zeros((NTILES, 32, 32), dtype=np.int64)
+    for t in range(NTILES):
         b = raw[t * TILE_BYTES:(t + 1) * TILE_BYTES][off]
         tiles[t] = b.view(np.int8) if t & 1 else b
     return tiles
@@ -163,3 +166,108 @@ def test_stage_a_operand_reads_stay_in_its_quarter():
                 # coefficient of the natural row behind it
                 assert (64 * (m // 4) * 2 + logical) // 2 == 16 * m + k // 2
         assert start % 16 == 0
+
+
+def model_forward(tiles: np.ndarray, x: np.ndarray):
+    """The forward kernel's arithmetic: stage 1 per coefficient c from the
+    transposed operand (K byte 2m + b = byte b of X[m][c]), stage 2 per block
+    i from the bytes of the int32 stage-1 sums, exact reduction to [0, q)."""
+    n = x.shape[0]
+    X = np.ascontiguousarray(x.astype(np.int16)).reshape(n, 16, 16)   # [p][m][c]
+    S1 = np.zeros((n, 16, 16), dtype=np.int64)                          # [p][i][c]
+    for c in range(16):
+        col = np.ascontiguousarray(X[:, :, c]).view(np.uint8).reshape(n, 32)
+        d = as_u8(col) @ tiles[36].T + as_s8(col) @ tiles[37].T
+        assert np.abs(d).max() < 2 ** 31
+        S1[:, :, c] = d[:, :16] + 128 * d[:, 16:]
+    s32 = S1.astype(np.int32)
+    S2 = np.zeros((n, 16, 16), dtype=np.int64)                          # [p][i][c']
+    for i in range(16):
+        by = s32[:, i, :].copy().view(np.uint8).reshape(n, 64)          # byte j of S[c] at 4c + j
+        d = np.zeros((n, 32), dtype=np.int64)
+        for h in range(2):
+            kb = by[:, 32 * h:32 * h + 32]
+            t = 38 + 4 * i + 2 * h
+            d += as_u8(kb) @ tiles[t].T + as_s8(kb) @ tiles[t + 1].T
+        assert np.abs(d).max() < 2 ** 31
+        S2[:, i] = d[:, :16] + 128 * d[:, 16:]
+    quot = (S2 * M40 + Q * 65536 * M40) >> 40
+    r = (S2 - quot * Q) & 0xFFFF
+    return r.astype(np.int16).reshape(n, 256), S1, S2
+
+
+def test_forward_tables_hold_the_stage_matrices(tk):
+    tiles = decode(tk.get_table(8))
+    m1 = tk.get_table(0).astype(np.int64)       # [i][m]
+    m2 = tk.get_table(1).astype(np.int64)       # [block][out][in]
+
+    def limbs(v):
+        return np.concatenate([v & 127, v >> 7])
+    assert (tiles[36][:, 1::2] == 0).all() and (tiles[37][:, 0::2] == 0).all()
+    assert (tiles[36][:, 0::2] == limbs(m1)).all()
+    assert (tiles[37][:, 1::2] == limbs(256 * m1 % Q)).all()
+    for i in range(16):
+        for h in range(2):
+            for cc in range(8):
+                for j in range(4):
+                    col = m2[i][:, 8 * h + cc] * pow(256, j, Q) % Q
+                    u, s = tiles[38 + 4 * i + 2 * h][:, 4 * cc + j], tiles[39 + 4 * i + 2 * h][:, 4 * cc + j]
+                    assert (u == (limbs(col) if j < 3 else 0)).all()
+                    assert (s == (limbs(col) if j == 3 else 0)).all()
+
+
+def test_forward_model_matches_the_oracle_and_bounds_hold(tk, oracle):
+    tiles = decode(tk.get_table(8))
+    x = inputs()
+    out, S1, S2 = model_forward(tiles, x)
+    assert S1.min() >= -(2 ** 24) and S1.max() < 2 ** 25
+    assert S2.min() >= -(2 ** 16) and S2.max() < 2 ** 26
+    assert out.min() >= 0 and out.max() < Q
+    assert (out == canon(oracle.ntt(canon(x).astype(np.int16)))).all()
+
+
+def test_forward_transposition_layout():
+    """In-place transposition of a loaded tile: warp half h reads chunk 2m + h
+    (coefficients 8h .. 8h+7 of block m) of its row from the swizzled slot and
+    writes c-tile c = 8h + cc at 4096 c + (p / 8) 256 + (p % 8) 16 + 128 kc,
+    K bytes 16 kc .. 16 kc + 15 = blocks 8 kc .. 8 kc + 7 of coefficient c.
+    Checked: the reads cover the slot once, the writes cover it once, and a
+    K-major no-swizzle descriptor (LBO 128, SBO 256) at 4096 c reads back
+    X[m][c] for K byte 2m + b of row p."""
+    reads = np.zeros(65536, dtype=np.int64)
+    writes = np.zeros(65536, dtype=np.int64)
+    for p in range(128):
+        for h in range(2):
+            for m in range(16):
+                k = 2 * m + h
+                a = (k >> 3) * 16384 + p * 128 + (((k & 7) ^ (p & 7)) << 4)
+                reads[a:a + 16] += 1
+            for cc in range(8):
+                c = 8 * h + cc
+                for kc in range(2):
+                    a = 4096 * c + (p >> 3) * 256 + (p & 7) * 16 + 128 * kc
+                    writes[a:a + 16] += 1
+                    for kb in range(16):        # descriptor view of the same byte
+                        kbyte = 16 * kc + kb
+                        d = 4096 * c + (p // 8) * 256 + (kbyte // 16) * 128 + (p % 8) * 16 + kbyte % 16
+                        assert d == a + kb
+                        assert kbyte // 2 < 16                      # block m = kbyte / 2
+    assert (reads == 1).all() and (writes == 1).all()
+
+
+def test_forward_output_addresses_are_the_tma_swizzle_layout():
+    """Block i of row p (coefficients 16 i .. 16 i + 15) goes to natural chunks
+    2i and 2i + 1 through the swizzle: the two 16-byte stores per block cover
+    the slot once and agree with TMA's placement of each coefficient."""
+    seen = np.zeros(65536, dtype=np.int64)
+    for p in range(128):
+        for i in range(16):
+            for half in range(2):
+                k = 2 * i + half
+                a = (k >> 3) * 16384 + p * 128 + (((k & 7) ^ (p & 7)) << 4)
+                for u in range(8):
+                    e = 16 * i + 8 * half + u
+                    w = 2 * (e % 64)
+                    assert a + 2 * u == (e // 64) * 16384 + p * 128 + (((w // 16) ^ (p % 8)) << 4) + w % 16
+                seen[a:a + 16] += 1
+    assert (seen == 1).all()
