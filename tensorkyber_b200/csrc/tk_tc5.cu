@@ -164,8 +164,8 @@ __device__ __forceinline__ uint32_t sw128_chunk(uint32_t slot, uint32_t p, uint3
 //     order (K byte 2m + b), K-major without swizzle (8-row core matrices of
 //     16-byte rows, the two K halves 128 bytes apart, 8-row groups 256 bytes
 //     apart); warp w reads coefficients 8 (w / 4) .. + 7 of every block of its
-//     rows, a CTA-wide barrier of those warps, then every warp writes its
-//     c-tiles;
+//     rows, the 8 warps meet on an mbarrier (bounded wait), then every warp
+//     writes its c-tiles over the rows;
 //   * stage 1 (M1 over m): per c-tile one unsigned and one signed MMA from
 //     shared memory, chunks of c-tiles {0-3}, {4-7}, {8-11}, {12-15}; its
 //     sums go to tensor memory as column 16 i + c (block i, coefficient c);
