@@ -215,14 +215,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
     tmem_alloc(base + L::kOffTmemSlot, kTmemCols);
     tmem_relinquish();
   }
+  tc_fence_before();
+  __syncthreads();  // the mbarriers are initialised (and fenced) before any use
+  tc_fence_after();
+  const uint32_t tmem = *(volatile uint32_t*)(basep + L::kOffTmemSlot);
   if (warp == kTcTmaWarp && lane == 0) {  // constant tiles (written once by the host)
     mbar_expect_tx(consts, L::kTableBytes);
     bulk_g2s(tables, P.tables, L::kTableBytes, consts);
   }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *(volatile uint32_t*)(basep + L::kOffTmemSlot);
   // the tile data may have been written by the previous kernel in the stream
   grid_dependency_wait();
   grid_launch_dependents();
