@@ -35,7 +35,9 @@ def jobs(seed, k, n, with_e=True):
     r = rng(seed)
     A = r.integers(0, Q, size=(n, k, k, 256)).astype(np.int16)
     s = r.integers(-32768, 32768, size=(n, k, 256)).astype(np.int16)
-    e = r.integers(-32768, 32768, size=(n, k, 256)).astype(np.int16) if with_e else None
+    # e is added to the inverse's output with int16 wrap-around (as the
+    # reference's polynomial add): noise-sized, so neither side's sum wraps
+    e = r.integers(-3, 4, size=(n, k, 256)).astype(np.int16) if with_e else None
     return A, s, e
 
 
