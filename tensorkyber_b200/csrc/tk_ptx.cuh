@@ -266,6 +266,12 @@ __device__ __forceinline__ void tc_ld64(uint32_t taddr, uint32_t (&r)[64]) {
         "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
       : "r"(taddr));
 }
+// 2 consecutive 32-bit columns of this thread's lane.
+__device__ __forceinline__ void tc_st2(uint32_t taddr, uint32_t a, uint32_t b) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(taddr), "r"(a),
+               "r"(b)
+               : "memory");
+}
 // 4 consecutive 32-bit columns of this thread's lane.
 __device__ __forceinline__ void tc_st4(uint32_t taddr, uint32_t a, uint32_t b, uint32_t c,
                                        uint32_t d) {

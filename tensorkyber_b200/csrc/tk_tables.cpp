@@ -260,40 +260,23 @@ void build_tc5_tables(const Matrices& M, uint8_t* out) {
   auto put = [&](int tile, int n, int k, int64_t v) {
     out[tile * kTc5TileBytes + tc5_tile_offset(n, k)] = (uint8_t)v;
   };
-  for (int m = 0; m < 16; m++)
-    for (int o = 0; o < 16; o++)
-      for (int g = 0; g < 2; g++)
-        for (int ci = 0; ci < 16; ci++) {
-          put(2 * m, o + 16 * g, 2 * ci, limb(M.ma[m][o][ci], g));
-          put(2 * m + 1, o + 16 * g, 2 * ci + 1, limb(byte_weighted(M.ma[m][o][ci], 1), g));
-        }
-  for (int h = 0; h < 2; h++)
-    for (int i = 0; i < 16; i++)
-      for (int g = 0; g < 2; g++)
-        for (int mm = 0; mm < 8; mm++) {
-          const int m = 8 * h + mm;
-          for (int j = 0; j < 3; j++)
-            put(32 + 2 * h, i + 16 * g, 4 * mm + j, limb(byte_weighted(M.minv[i][m], j), g));
-          put(32 + 2 * h + 1, i + 16 * g, 4 * mm + 3, limb(byte_weighted(M.minv[i][m], 3), g));
-        }
-  for (int i = 0; i < 16; i++)
+  for (int o = 0; o < 16; o++)
     for (int g = 0; g < 2; g++)
-      for (int m = 0; m < 16; m++) {
-        put(36, i + 16 * g, 2 * m, limb(M.m1[i][m], g));
-        put(37, i + 16 * g, 2 * m + 1, limb(byte_weighted(M.m1[i][m], 1), g));
-      }
-  for (int i = 0; i < 16; i++)
-    for (int h = 0; h < 2; h++)
-      for (int o = 0; o < 16; o++)
-        for (int g = 0; g < 2; g++)
-          for (int cc = 0; cc < 8; cc++) {
-            const int c = 8 * h + cc;
-            for (int j = 0; j < 3; j++)
-              put(38 + 4 * i + 2 * h, o + 16 * g, 4 * cc + j,
-                  limb(byte_weighted(M.m2[i][o][c], j), g));
-            put(38 + 4 * i + 2 * h + 1, o + 16 * g, 4 * cc + 3,
-                limb(byte_weighted(M.m2[i][o][c], 3), g));
+      for (int j = 0; j < 16; j++)
+        for (int b = 0; b < 2; b++) {
+          // inverse stage A, every block m: input coefficient j
+          for (int m = 0; m < 16; m++) {
+            if (b == 0) put(2 * m, o + 16 * g, 2 * j, limb(M.ma[m][o][j], g));
+            else put(2 * m + 1, o + 16 * g, 2 * j + 1, limb(byte_weighted(M.ma[m][o][j], 1), g));
           }
+          // inverse stage B: input block j, byte b
+          put(32, o + 16 * g, 2 * j + b, limb(byte_weighted(M.minv[o][j], b), g));
+          // forward stage 1: input block j, byte b (unsigned low / signed high)
+          put(33 + b, o + 16 * g, 2 * j + b, limb(byte_weighted(M.m1[o][j], b), g));
+          // forward stage 2, block i: input coefficient j, byte b
+          for (int i = 0; i < 16; i++)
+            put(35 + i, o + 16 * g, 2 * j + b, limb(byte_weighted(M.m2[i][o][j], b), g));
+        }
 }
 
 }  // namespace tk

@@ -122,33 +122,30 @@ void build_pair_roots(int32_t z[128]);
 // built from M compute f * invntt.
 void scale_inverse(Matrices* M, int64_t f);
 
-// B operands of the TMEM inverse (tk_tc5.cu), one 1 KiB tile per MMA shape:
-// N = 32 rows (n = out + 16 * limb: output coefficient, 7-bit limb of the
-// constant) x K = 32 bytes, int8 values, in the tcgen05 K-major layout
+// B operands of the tcgen05 kernels (tk_tc5.cu), one 1 KiB tile per MMA
+// shape: N = 32 rows (n = out + 16 * limb: output coefficient, 7-bit limb of
+// the constant) x K = 32 bytes, int8 values, in the tcgen05 K-major layout
 // without swizzle: row n, K byte k at (n / 8) * 256 + (k / 16) * 128 +
 // (n % 8) * 16 + k % 16 (8-row core matrices of 16 bytes per row; the two
 // K halves 128 bytes apart, 8-row groups 256 bytes apart).
-//   tile 2m + t      stage A (MA of block m): K byte k = 2 c' + b, byte b of
-//                    input coefficient c'.  t = 0 (unsigned data): the low
-//                    bytes, constant MA[m][out][c']; t = 1 (signed data): the
-//                    high bytes, constant 256 MA[m][out][c'] mod q; the other
-//                    byte's rows are zero.
-//   tile 32 + 2h + t stage B (Minv), K step h: K byte k = 4 (m - 8h) + j,
-//                    byte j of the int32 stage-A sum of block m.  t = 0
-//                    (unsigned): bytes 0-2, constant Minv[out][m] 256^j mod
-//                    q; t = 1 (signed): byte 3, constant Minv[out][m] 2^24
-//                    mod q; the other bytes' rows are zero.
-//   tile 36 + t      forward stage 1 (M1): K byte k = 2 m + b, byte b of the
+//   tile 2m + t      inverse stage A (MA of block m): K byte k = 2 c' + b,
+//                    byte b of input coefficient c'.  t = 0 (unsigned data):
+//                    the low bytes, constant MA[m][out][c']; t = 1 (signed
+//                    data): the high bytes, constant 256 MA[m][out][c'] mod
+//                    q; the other byte's rows are zero.
+//   tile 32          inverse stage B (Minv): K byte k = 2 m + b, byte b of
+//                    the (non-negative, below 2^12) stage-A value of block m;
+//                    constant Minv[out][m] 256^b mod q.
+//   tile 33 + t      forward stage 1 (M1): K byte k = 2 m + b, byte b of the
 //                    block-m coefficient; t = 0: low bytes, constant
 //                    M1[out][m]; t = 1: high bytes, 256 M1[out][m] mod q.
-//   tile 38 + 4i + 2h + t  forward stage 2 (M2 of block i), K step h: K byte
-//                    k = 4 (c - 8h) + j, byte j of the int32 stage-1 sum of
-//                    coefficient c; t = 0: bytes 0-2, constant M2[i][out][c]
-//                    256^j mod q; t = 1: byte 3, M2[i][out][c] 2^24 mod q.
-// The inverse uses tiles 0-35, the forward tiles 36-101.
+//   tile 35 + i      forward stage 2 (M2 of block i): K byte k = 2 c + b,
+//                    byte b of the (non-negative, below 2^12) stage-1 value
+//                    of coefficient c; constant M2[i][out][c] 256^b mod q.
+// The inverse uses tiles 0-32, the forward tiles 33-50.
 constexpr int kTc5TileBytes = 1024;
-constexpr int kTc5InvTiles = 36;
-constexpr int kTc5FwdTiles = 66;
+constexpr int kTc5InvTiles = 33;
+constexpr int kTc5FwdTiles = 18;
 constexpr int kTc5Tiles = kTc5InvTiles + kTc5FwdTiles;
 constexpr int kTc5TableBytes = kTc5Tiles * kTc5TileBytes;
 inline int tc5_tile_offset(int n, int k) {

@@ -1,49 +1,53 @@
-// tk_tc5.cu -- batched ML-KEM inverse NTT on the 5th-generation tensor cores
-// (tcgen05.mma kind::i8, int32 accumulators in tensor memory), sm_100a.
+// tk_tc5.cu -- batched ML-KEM NTT and inverse NTT on the 5th-generation
+// tensor cores (tcgen05.mma kind::i8, int32 accumulators in tensor memory),
+// sm_100a.
 //
-// Same transform as the mma.sync inverse (tk_ntt_mma.cu) and the same method
-// (TensorKyber's intt_core, ntt_bench/ntt_kernels.cuh:548-625): stage A
-// applies the per-block matrices MA^(m) (Gentleman-Sande layers len 2..8),
-// stage B the 16x16 matrix Minv over the block index m (layers len 16..128
-// and the final x1441 Montgomery factor), every constant as two 7-bit int8
-// limbs.  The B200 formulation:
+// Same transforms as the mma.sync kernels (tk_ntt_mma.cu) and the same method
+// (TensorKyber's ntt_core / intt_core, ntt_bench/ntt_kernels.cuh:393-489,
+// 548-625): forward layers 1-4 as M1 over the block index m, layers 5-7 as the
+// per-block M2^(i); inverse stage A as the per-block MA^(m), stage B as Minv
+// over m (with the final x1441 Montgomery factor); every constant as two
+// 7-bit int8 limbs.  The B200 formulation:
 //
 //   * A tile is 128 polynomials, the M dimension of every MMA (one polynomial
 //     per tensor-memory lane).  TMA loads it as four boxes of 64 coefficients
 //     x 128 rows with the 128-byte swizzle, which is exactly the canonical
-//     K-major SW128 operand layout: stage A's A operand for block m is the
-//     32 bytes of that block in each row, read straight from the loaded tile.
+//     K-major SW128 operand layout: the inverse's stage-A A operand for block
+//     m is the 32 bytes of that block in each row, read straight from the
+//     loaded tile.  The forward contracts over m first, so the 8 epilogue
+//     warps transpose the tile in place into stage 1's operand (K-major
+//     without swizzle) before its MMAs.
 //   * Signed data need no CUDA-core pass.  An int16 x = b0 + 256 b1 with b0
-//     unsigned and b1 signed, so stage A is two MMAs per block into the same
-//     accumulator: one with unsigned data and constants on the low bytes'
-//     K rows (MA), one with signed data and constants on the high bytes' K rows
-//     (256 MA mod q); the other rows of each constant tile are zero.
-//   * Stage A's accumulators (lo / hi constant limb) are combined into the
-//     int32 sum S = D_lo + 128 D_hi (one IMAD) and written back to tensor
-//     memory transposed: column 16 c + m holds S of block m, coefficient c.
-//     Stage B's A operand for coefficient c is then columns 16 c .. 16 c + 15
-//     straight from tensor memory (K byte 4 (m - 8h) + j = byte j of S[m]),
-//     again split in two MMA kinds: bytes 0-2 unsigned, byte 3 signed, so S is
-//     taken exactly as two's complement and never reduced in between.
-//   * Stage B's sums S (in [-2^16, 2^26)) get one centred exact reduction and
-//     are packed to int16, written in the same swizzled layout over the tile's
-//     own input slot (its MMAs have finished), and TMA stores the tile.
+//     unsigned and b1 signed, so the first stage is two MMAs per block (or
+//     coefficient) into the same accumulator: one with unsigned data and
+//     constants on the low bytes' K rows, one with signed data and constants
+//     256 C mod q on the high bytes' K rows; the other rows of each constant
+//     tile are zero.
+//   * The first stage's sums S = D_lo + 128 D_hi get one lazy reduction to
+//     [0, q + 11) and go back to tensor memory packed two to a 32-bit column,
+//     transposed: output n's second-stage operand is the 8 columns 8 n .. 8 n
+//     + 7, read by tcgen05.mma straight from tensor memory, one unsigned MMA
+//     per coefficient (inverse) or block (forward).
+//   * The second stage's sums (below 2^24) get one exact reduction (centred
+//     for the inverse, [0, q) for the forward), are packed to int16 and
+//     written in the TMA layout over the tile's own input slot (its MMAs have
+//     finished), and TMA stores the tile.
 //
 // Roles (320 threads, one CTA per SM by shared memory): warp 9 lane 0 issues
 // TMA loads and stores; warp 8 lane 0 issues MMAs (and warp 8 owns the
 // tensor-memory allocation); warps 0-7 move data between tensor memory,
 // registers and shared memory, warps w and w + 4 sharing tensor-memory lanes
 // 32 (w % 4) .. + 31 (polynomials) and splitting the columns.  Tensor memory
-// (512 columns): 0-255 the transposed stage-A sums, 256-383 and 384-511 two
+// (512 columns): 0-127 the packed first-stage values, 256-383 and 384-511 two
 // accumulator buffers of four 32-column MMA results each.  Per tile the MMA
-// thread issues 8 chunks (stage A blocks 0-3, 4-7, 8-11, 12-15, then stage B
-// coefficient sets {0-3}, {8-11}, {4-7}, {12-15}) into the buffers in turn;
-// warps 0-3 take buffer 0, warps 4-7 buffer 1.  Two input slots of 64 KiB:
-// the load of tile k + 2 goes into tile k's slot once tile k's output
-// (written over its input) has been read out by the store.  Every mbarrier
-// wait gives up after 2 s (status bit 1, as the other inverse kernels); the
-// MMA thread then drains its MMAs and the producer its copies before the
-// CTA frees tensor memory and exits.
+// thread issues 8 chunks of four MMA results (first stage: 8 MMAs each;
+// second stage: 4 each) into the buffers in turn; warps 0-3 take buffer 0,
+// warps 4-7 buffer 1.  Two input slots of 64 KiB: the load of tile k + 2 goes
+// into tile k's slot once tile k's output (written over its input) has been
+// read out by the store.  Every mbarrier wait gives up after 2 s (status bit
+// 0 forward / 1 inverse, as the other kernels); the MMA thread then drains
+// its MMAs and the producer its copies before the CTA frees tensor memory and
+// exits.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
@@ -91,10 +95,12 @@ constexpr uint32_t kColD0 = 256;  // accumulator buffer b at kColD0 + 128 b
 constexpr uint32_t kIdescU8 = (2u << 4) | (4u << 17) | (8u << 24);
 constexpr uint32_t kIdescS8 = kIdescU8 | (1u << 7) | (1u << 10);
 constexpr uint64_t kWaitNs = 2000000000ull;
-// exact reductions of the second stage's sums (red_*_wide below)
-constexpr int64_t kM40 = 330282857;  // ceil(2^40 / q) = floor(2^40 / q) + 1
-constexpr int64_t kAddCentred40 = (3329ll * 65536 + 1664) * kM40;
-constexpr int64_t kAddExact40 = (3329ll * 65536) * kM40;
+// The first stage's sums S (in [-16 * 128 (q-1), 16 * 382 (q-1)]: unsigned
+// low bytes and signed high bytes against constants below q) plus this
+// multiple of q are non-negative and below 2^25, where red_lazy leaves
+// [0, q + 11) (floor(2^32 / q) is 0.406 below 2^32 / q: the quotient is one
+// short only when T mod q < 0.406 q T / 2^32 < 10.6), high byte <= 13.
+constexpr uint32_t kFirstBias = 2048u * 3329u;
 
 __device__ __align__(128) uint8_t g_tc5_tables[kTc5TableBytes];
 
@@ -106,23 +112,6 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | ((uint64_t)layout << 61);
 }
 constexpr uint32_t kLayoutNone = 0, kLayoutSw128 = 2;
-
-// S in [-2^16, 2^26): an int32 whose low 16 bits are the centred residue of S
-// in [-(q-1)/2, (q-1)/2].  T = S + q 2^16 (a multiple of q and of 2^16) lies
-// in [0, 2^28); floor((T + (q-1)/2) / q) = ((T + 1664) ceil(2^40/q)) >> 40
-// exactly there (the multiplier's error adds < 2^28 / 2^40 < 1/q), as one
-// 64-bit multiply-add; S - q quot differs from T - q quot by q 2^16.
-__device__ __forceinline__ uint32_t red_centred_wide(uint32_t s) {
-  const int64_t x = (int64_t)(int32_t)s * kM40 + kAddCentred40;
-  const uint32_t quot = (uint32_t)((uint64_t)x >> 40);
-  return s - quot * 3329u;
-}
-// The same for the canonical residue in [0, q): floor(T / q).
-__device__ __forceinline__ uint32_t red_exact_wide(uint32_t s) {
-  const int64_t x = (int64_t)(int32_t)s * kM40 + kAddExact40;
-  const uint32_t quot = (uint32_t)((uint64_t)x >> 40);
-  return s - quot * 3329u;
-}
 
 __device__ __forceinline__ void st_shared_v2(uint32_t addr, uint32_t a, uint32_t b) {
   asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(addr), "r"(a), "r"(b) : "memory");
@@ -157,23 +146,17 @@ __device__ __forceinline__ uint32_t sw128_chunk(uint32_t slot, uint32_t p, uint3
   return slot + (k >> 3) * kTcQuarterBytes + p * 128u + (((k & 7u) ^ (p & 7u)) << 4);
 }
 
-// kInverse: see the file comment.  Forward (the same roles and pipeline):
-//   * the 8 epilogue warps first transpose the loaded tile in place into
-//     stage 1's A operand: for coefficient c (c-tile c, 4 KiB at 4096 c of
-//     the slot), row p's 32 K bytes are the blocks' values X[m][c] in block
-//     order (K byte 2m + b), K-major without swizzle (8-row core matrices of
-//     16-byte rows, the two K halves 128 bytes apart, 8-row groups 256 bytes
-//     apart); warp w reads coefficients 8 (w / 4) .. + 7 of every block of its
-//     rows, the 8 warps meet on an mbarrier (bounded wait), then every warp
-//     writes its c-tiles over the rows;
-//   * stage 1 (M1 over m): per c-tile one unsigned and one signed MMA from
-//     shared memory, chunks of c-tiles {0-3}, {4-7}, {8-11}, {12-15}; its
-//     sums go to tensor memory as column 16 i + c (block i, coefficient c);
-//   * stage 2 (M2^(i) of block i): four MMAs per block from tensor-memory
-//     columns 16 i .. 16 i + 15 (bytes 0-2 unsigned, byte 3 signed) against
-//     the block's own constant tiles, chunks of blocks {0-3}, {4-7}, ...;
-//     exact reduction to [0, q), natural-order rows written to the slot in
-//     the TMA layout (two 16-byte chunks per block).
+// The forward's transposition: for coefficient c (c-tile c, 4 KiB at 4096 c
+// of the slot), row p's 32 K bytes are the blocks' values X[m][c] in block
+// order (K byte 2m + b), K-major without swizzle (8-row core matrices of
+// 16-byte rows, the two K halves 128 bytes apart, 8-row groups 256 bytes
+// apart).  Warp w reads coefficients 8 (w / 4) .. + 7 of every block of its
+// rows, the 8 warps meet on an mbarrier (bounded wait), then every warp writes
+// its c-tiles over the rows.  Stage 1 runs per c-tile in chunks of c-tiles
+// {0-3}, {4-7}, ..., stage 2 per block i from tensor-memory columns 8 i ..
+// 8 i + 7 against the block's own constant tile, chunks of blocks {0-3},
+// {4-7}, ...; its rows (two 16-byte chunks per block) go to the slot in the
+// TMA layout.
 template <bool kInverse>
 __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ Tc5Params P) {
   using L = Tc5Layout<kInverse>;
@@ -301,8 +284,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
               tc_mma_ss(d, a, tile_desc(2 * idx + 1), kIdescS8, 1);
             } else {
               const uint64_t a = smem_desc(slot_addr(s) + 4096u * idx, 128, 256, kLayoutNone);
-              tc_mma_ss(d, a, tile_desc(36), kIdescU8, 0);
-              tc_mma_ss(d, a, tile_desc(37), kIdescS8, 1);
+              tc_mma_ss(d, a, tile_desc(33), kIdescU8, 0);
+              tc_mma_ss(d, a, tile_desc(34), kIdescS8, 1);
             }
           }
           tc_commit(d_full(b));
@@ -316,18 +299,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
         for (int j = 0; j < 4 && ok; j++) {
           const int b = j & 1;
           if (!(ok = take(b))) break;
+          // inverse: coefficient sets {0-3}, {8-11}, {4-7}, {12-15} (buffer 0,
+          // warps 0-3: 0-7; buffer 1, warps 4-7: 8-15); forward: blocks 4j ..
           const int first = kInverse ? 8 * (j & 1) + 4 * (j >> 1) : 4 * j;
 #pragma unroll
           for (int u = 0; u < 4; u++) {
             const int idx = first + u;
             const uint32_t d = tmem + kColD0 + 128u * b + 32u * u;
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-              const uint32_t a = tmem + kColY + 16u * idx + 8u * h;
-              const int tl = kInverse ? 32 + 2 * h : 38 + 4 * idx + 2 * h;
-              tc_mma_ts(d, a, tile_desc(tl), kIdescU8, h);
-              tc_mma_ts(d, a, tile_desc(tl + 1), kIdescS8, 1);
-            }
+            tc_mma_ts(d, tmem + kColY + 8u * idx, tile_desc(kInverse ? 32 : 35 + idx), kIdescU8,
+                      0);
           }
           tc_commit(d_full(b));
           use[b]++;
@@ -392,8 +372,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
         __syncwarp();
         if (lane == 0) mbar_arrive(x_ready);
       }
-      // first stage's sums -> tensor memory column 16 n + idx (n: the MMA's
-      // output column, idx: its position in the chunk), chunks j = half, half + 2
+      // first stage: S = D_lo + 128 D_hi, lazily reduced to [0, q + 11), packed
+      // in pairs of consecutive MMA results (idx 4j + u): tensor-memory column
+      // 8 n + 2 j + u / 2 of output n holds results 4j + u, 4j + u + 1 (the
+      // second stage's K bytes 4 (2j + u/2) .. + 3), chunks j = half, half + 2
 #pragma unroll 1
       for (int jj = 0; jj < 2; jj++) {
         const int j = half + 2 * jj;
@@ -407,9 +389,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
         tc_wait_ld();
         give_back();
 #pragma unroll
-        for (int n = 0; n < 16; n++)
-          tc_st4(ycol + 16u * n + 4u * j, r0[n] + (r0[16 + n] << 7), r0[32 + n] + (r0[48 + n] << 7),
-                 r1[n] + (r1[16 + n] << 7), r1[32 + n] + (r1[48 + n] << 7));
+        for (int n = 0; n < 16; n++) {
+          const uint32_t v0 = red_lazy(r0[n] + (r0[16 + n] << 7) + kFirstBias);
+          const uint32_t v1 = red_lazy(r0[32 + n] + (r0[48 + n] << 7) + kFirstBias);
+          const uint32_t v2 = red_lazy(r1[n] + (r1[16 + n] << 7) + kFirstBias);
+          const uint32_t v3 = red_lazy(r1[32 + n] + (r1[48 + n] << 7) + kFirstBias);
+          tc_st2(ycol + 8u * n + 2u * j, pack2(v0, v1), pack2(v2, v3));
+        }
       }
       if (!ok) break;
       tc_wait_st();
@@ -424,26 +410,28 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
           ok = false;
           break;
         }
-        uint32_t r0[64], r1[64];
-        tc_ld64(dcol, r0);
-        tc_ld64(dcol + 64, r1);
-        tc_wait_ld();
-        give_back();
         if (kInverse) {
-          // coefficients 16 i + c0 .. +3 of every block i: 8 bytes at byte
-          // 2 c0 % 16 of 16-byte chunk 2 i + c0 / 8
-          const int c0 = 8 * (j & 1) + 4 * (j >> 1);
+          // coefficients 16 i + c0 .. +3 of every block i (c0 = 8 half + 4 jj):
+          // 8 bytes at byte 8 jj of 16-byte chunk 2 i + half
+          uint32_t r0[64], r1[64];
+          tc_ld64(dcol, r0);
+          tc_ld64(dcol + 64, r1);
+          tc_wait_ld();
+          give_back();
 #pragma unroll
           for (int i = 0; i < 16; i++) {
-            const uint32_t z0 = red_centred_wide(r0[i] + (r0[16 + i] << 7));
-            const uint32_t z1 = red_centred_wide(r0[32 + i] + (r0[48 + i] << 7));
-            const uint32_t z2 = red_centred_wide(r1[i] + (r1[16 + i] << 7));
-            const uint32_t z3 = red_centred_wide(r1[32 + i] + (r1[48 + i] << 7));
-            st_shared_v2(sw128_chunk(slot, p, 2u * i + (uint32_t)(c0 >> 3)) +
-                             8u * ((uint32_t)(c0 >> 2) & 1u),
-                         pack2(z0, z1), pack2(z2, z3));
+            const uint32_t w0 = pack2(red_centred(r0[i] + (r0[16 + i] << 7)),
+                                      red_centred(r0[32 + i] + (r0[48 + i] << 7)));
+            const uint32_t w1 = pack2(red_centred(r1[i] + (r1[16 + i] << 7)),
+                                      red_centred(r1[32 + i] + (r1[48 + i] << 7)));
+            st_shared_v2(sw128_chunk(slot, p, 2u * i + half) + 8u * jj, w0, w1);
           }
         } else {
+          uint32_t r0[64], r1[64];
+          tc_ld64(dcol, r0);
+          tc_ld64(dcol + 64, r1);
+          tc_wait_ld();
+          give_back();
           // blocks 4j .. 4j+3, each 16 coefficients = two 16-byte chunks
 #pragma unroll
           for (int u = 0; u < 4; u++) {
@@ -451,8 +439,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
             uint32_t w[8];
 #pragma unroll
             for (int t = 0; t < 8; t++)
-              w[t] = pack2(red_exact_wide(r[2 * t] + (r[16 + 2 * t] << 7)),
-                           red_exact_wide(r[2 * t + 1] + (r[17 + 2 * t] << 7)));
+              w[t] = pack2(red_exact(r[2 * t] + (r[16 + 2 * t] << 7)),
+                           red_exact(r[2 * t + 1] + (r[17 + 2 * t] << 7)));
             const uint32_t i = 4u * j + u;
             st_shared_v4(sw128_chunk(slot, p, 2u * i), w[0], w[1], w[2], w[3]);
             st_shared_v4(sw128_chunk(slot, p, 2u * i + 1), w[4], w[5], w[6], w[7]);

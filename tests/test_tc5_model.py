@@ -1,35 +1,36 @@
 """CPU model of the tcgen05 kernels (tensorkyber_b200/csrc/tk_tc5.cu).
 
 The library's own B-operand tiles (table 8) are decoded from the tcgen05
-K-major layout and pushed through the kernel's integer steps with numpy: stage
-A as a pair of MMAs per block (unsigned data against the low-byte constants,
-signed data against the high-byte constants) into one int32 accumulator per
-constant limb, the recombination S = D_lo + 128 D_hi, stage B over the four
-bytes of each stage-A sum (bytes 0-2 unsigned, byte 3 signed) and the 40-bit
-centred reduction.  Every coefficient must agree with the oracle mod q, the
-intermediate bounds the kernel relies on must hold, and the shared-memory
-addresses the kernel writes its output to must be the TMA 128-byte-swizzle
-layout of the tile (the layout its loads and stores use).  No GPU needed."""
+K-major layout and pushed through the kernels' integer steps with numpy: the
+first stage as a pair of MMAs per block or coefficient (unsigned data against
+the low-byte constants, signed data against the high-byte constants) into one
+int32 accumulator per constant limb, the recombination S = D_lo + 128 D_hi, a
+lazy reduction of S + 2048 q to [0, q + 11), the second stage as one unsigned
+MMA over the two bytes of those values, and the exact (forward) or centred
+(inverse) reduction.  Every coefficient must agree with the oracle mod q, the
+intermediate bounds the kernels rely on must hold, and the shared-memory
+addresses they read and write must be the TMA 128-byte-swizzle layout of the
+tile (the layout its loads and stores use).  No GPU needed."""
 import numpy as np
 
 from conftest import rng
 from py_oracle import Q, canon
 
-M40 = 330282857                      # ceil(2^40 / q)
-ADD40 = (Q * 65536 + 1664) * M40
 TILE_BYTES = 1024
+NTILES = 51           # 0-32 the inverse's, 33-50 the forward's
+FIRST_BIAS = 2048 * Q
+BAR_LAZY = 1290167    # floor(2^32 / q)
+BAR_EXACT = 82570715  # ceil(2^38 / q)
 
 
 def tile_offset(n, k):
     return (n >> 3) * 256 + (k >> 4) * 128 + (n & 7) * 16 + (k & 15)
 
 
-NTILES = 102          # 0-35 the inverse's, 36-101 the forward's
-
-
 def decode(raw: np.ndarray) -> np.ndarray:
     """The tiles of B[n][k] (n = out + 16 limb, k = K byte), each read back from
-    the K-major core-matrix layout; even tiles as unsigned, odd as signed."""
+    the K-major core-matrix layout; the signed-data tiles (1, 3, .., 31 and
+    34) as signed bytes, the others unsigned."""
     raw = raw.view(np.uint8)
     assert raw.size == NTILES * TILE_BYTES
     off = np.array([[tile_offset(n, k) for k in range(32)] for n in range(32)])
@@ -37,7 +38,8 @@ def decode(raw: np.ndarray) -> np.ndarray:
     tiles = np.zeros((NTILES, 32, 32), dtype=np.int64)
     for t in range(NTILES):
         b = raw[t * TILE_BYTES:(t + 1) * TILE_BYTES][off]
-        tiles[t] = b.view(np.int8) if t & 1 else b
+        signed = (t < 32 and t & 1) or t == 34
+        tiles[t] = b.view(np.int8) if signed else b
     return tiles
 
 
@@ -49,33 +51,61 @@ def as_s8(a):
     return a.astype(np.uint8).view(np.int8).astype(np.int64)
 
 
+def red_lazy(t):
+    assert t.min() >= 0 and t.max() < 2 ** 25
+    return t - ((t * BAR_LAZY) >> 32) * Q
+
+
+def first_stage_values(d):
+    """[n][32] accumulators -> lazily reduced values [n][16] in [0, q + 11)."""
+    assert np.abs(d).max() < 2 ** 31
+    s = d[:, :16] + 128 * d[:, 16:]
+    assert s.min() >= -(2 ** 24) and s.max() < 2 ** 25
+    y = red_lazy(s + FIRST_BIAS)
+    assert y.min() >= 0 and y.max() < Q + 11
+    return y
+
+
+def second_stage(y_cols, tile):
+    """y_cols[n][16] values (K byte 2 v + b = byte b of value v) against one
+    unsigned tile -> S = D_lo + 128 D_hi [n][16], non-negative, < 2^24."""
+    by = np.stack([y_cols & 255, y_cols >> 8], axis=2).reshape(y_cols.shape[0], 32)
+    d = by @ tile.T
+    s = d[:, :16] + 128 * d[:, 16:]
+    assert s.min() >= 0 and s.max() < 2 ** 24
+    return s
+
+
 def model_inverse(tiles: np.ndarray, x: np.ndarray):
-    """The kernel's arithmetic on int16 rows x[n][256]; returns (int16 rows,
-    stage-A sums, stage-B sums)."""
     n = x.shape[0]
     raw = np.ascontiguousarray(x.astype(np.int16)).view(np.uint8).reshape(n, 16, 32)
-    SA = np.zeros((n, 16, 16), dtype=np.int64)          # [poly][m][c]
+    Y = np.zeros((n, 16, 16), dtype=np.int64)           # [poly][m][c]
     for m in range(16):
         d = as_u8(raw[:, m]) @ tiles[2 * m].T + as_s8(raw[:, m]) @ tiles[2 * m + 1].T
-        assert np.abs(d).max() < 2 ** 31
-        SA[:, m] = d[:, :16] + 128 * d[:, 16:]
-    assert SA.min() >= -2 ** 31 and SA.max() < 2 ** 31
-    sa32 = SA.astype(np.int32)
-    SB = np.zeros((n, 16, 16), dtype=np.int64)          # [poly][i][c]
+        Y[:, m] = first_stage_values(d)
+    out = np.zeros((n, 16, 16), dtype=np.int64)         # [poly][i][c]
     for c in range(16):
-        by = sa32[:, :, c].copy().view(np.uint8).reshape(n, 64)   # byte j of S[m] at 4m + j
-        d = np.zeros((n, 32), dtype=np.int64)
-        for h in range(2):
-            kb = by[:, 32 * h:32 * h + 32]
-            d += as_u8(kb) @ tiles[32 + 2 * h].T + as_s8(kb) @ tiles[33 + 2 * h].T
-        assert np.abs(d).max() < 2 ** 31
-        SB[:, :, c] = d[:, :16] + 128 * d[:, 16:]
-    xx = SB * M40 + ADD40
-    assert xx.min() >= 0 and xx.max() < 2 ** 63
-    quot = xx >> 40
-    r = (SB - quot * Q) & 0xFFFF
-    out = np.where(r >= 32768, r - 65536, r).astype(np.int16)
-    return out.reshape(n, 256), SA, SB
+        s = second_stage(Y[:, :, c], tiles[32])
+        quot = ((s * BAR_EXACT + 1664 * BAR_EXACT) >> 38)   # red_centred
+        out[:, :, c] = s - quot * Q
+    assert out.min() >= -(Q // 2) and out.max() <= Q // 2
+    return out.reshape(n, 256).astype(np.int16)
+
+
+def model_forward(tiles: np.ndarray, x: np.ndarray):
+    n = x.shape[0]
+    X = np.ascontiguousarray(x.astype(np.int16)).reshape(n, 16, 16)   # [p][m][c]
+    Y = np.zeros((n, 16, 16), dtype=np.int64)                         # [p][i][c]
+    for c in range(16):
+        col = np.ascontiguousarray(X[:, :, c]).view(np.uint8).reshape(n, 32)
+        d = as_u8(col) @ tiles[33].T + as_s8(col) @ tiles[34].T
+        Y[:, :, c] = first_stage_values(d)
+    out = np.zeros((n, 16, 16), dtype=np.int64)                       # [p][i][c']
+    for i in range(16):
+        s = second_stage(Y[:, i, :], tiles[35 + i])
+        out[:, i] = s - ((s * BAR_EXACT) >> 38) * Q                   # red_exact
+    assert out.min() >= 0 and out.max() < Q
+    return out.reshape(n, 256).astype(np.int16)
 
 
 def inputs():
@@ -87,48 +117,56 @@ def inputs():
     return np.concatenate([x, np.array(special)]).astype(np.int16)
 
 
+def limbs(v):
+    return np.concatenate([v & 127, v >> 7])
+
+
 def test_tables_hold_the_stage_matrices(tk):
-    """Decoded tiles: limbs of MA / 256 MA (stage A) and of Minv 256^j (stage
-    B) on their K rows, zero on the rows the other MMA kind covers."""
+    """Decoded tiles: limbs of the stage constants (times 256 on the high
+    bytes' K rows) and zeros on the rows the other MMA kind covers."""
     tiles = decode(tk.get_table(8))
+    m1 = tk.get_table(0).astype(np.int64)       # [i][m]
+    m2 = tk.get_table(1).astype(np.int64)       # [block][out][in]
     ma = tk.get_table(2).astype(np.int64)       # [m][out][in]
     minv = tk.get_table(3).astype(np.int64)     # [i][m]
-
-    def limbs(v):
-        return np.concatenate([v & 127, v >> 7])
     for m in range(16):
         assert (tiles[2 * m][:, 1::2] == 0).all() and (tiles[2 * m + 1][:, 0::2] == 0).all()
         assert (tiles[2 * m][:, 0::2] == limbs(ma[m])).all()
         assert (tiles[2 * m + 1][:, 1::2] == limbs(256 * ma[m] % Q)).all()
-    for h in range(2):
-        for mm in range(8):
-            for j in range(4):
-                col = minv[:, 8 * h + mm] * pow(256, j, Q) % Q
-                u, s = tiles[32 + 2 * h][:, 4 * mm + j], tiles[33 + 2 * h][:, 4 * mm + j]
-                assert (u == (limbs(col) if j < 3 else 0)).all()
-                assert (s == (limbs(col) if j == 3 else 0)).all()
+    assert (tiles[32][:, 0::2] == limbs(minv)).all()
+    assert (tiles[32][:, 1::2] == limbs(256 * minv % Q)).all()
+    assert (tiles[33][:, 1::2] == 0).all() and (tiles[34][:, 0::2] == 0).all()
+    assert (tiles[33][:, 0::2] == limbs(m1)).all()
+    assert (tiles[34][:, 1::2] == limbs(256 * m1 % Q)).all()
+    for i in range(16):
+        assert (tiles[35 + i][:, 0::2] == limbs(m2[i])).all()
+        assert (tiles[35 + i][:, 1::2] == limbs(256 * m2[i] % Q)).all()
 
 
-def test_model_matches_the_oracle_and_bounds_hold(tk, oracle):
-    tiles = decode(tk.get_table(8))
-    x = inputs()
-    out, SA, SB = model_inverse(tiles, x)
-    assert SA.min() >= -(2 ** 24) and SA.max() < 2 ** 25
-    assert SB.min() >= -(2 ** 16) and SB.max() < 2 ** 26     # red_centred_wide's domain
-    assert out.min() >= -(Q // 2) and out.max() <= Q // 2
-    want = oracle.invntt(canon(x).astype(np.int16))
-    assert (canon(out) == canon(want)).all()
+def test_inverse_model_matches_the_oracle(tk, oracle):
+    out = model_inverse(decode(tk.get_table(8)), inputs())
+    assert (canon(out) == canon(oracle.invntt(canon(inputs()).astype(np.int16)))).all()
 
 
-def test_centred_reduction_exact_on_its_domain():
-    s = np.concatenate([np.arange(-(2 ** 16), -(2 ** 16) + 100000),
-                        rng(5).integers(-(2 ** 16), 2 ** 26, size=2_000_000),
-                        np.arange(2 ** 26 - 100000, 2 ** 26)]).astype(np.int64)
-    quot = (s * M40 + ADD40) >> 40
-    r = (s - quot * Q) & 0xFFFF
-    got = np.where(r >= 32768, r - 65536, r)
-    t = s % Q
-    assert (got == np.where(t > Q // 2, t - Q, t)).all()
+def test_forward_model_matches_the_oracle(tk, oracle):
+    out = model_forward(decode(tk.get_table(8)), inputs())
+    assert (out == canon(oracle.ntt(canon(inputs()).astype(np.int16)))).all()
+
+
+def test_first_stage_bias_covers_the_sum_range():
+    """The first stage's sums lie in [-16 * 128 (q-1), 16 * 382 (q-1)]
+    (16 inputs of unsigned low and signed high bytes against constants below
+    q); adding 2048 q makes them non-negative and keeps them below 2^25, where
+    the lazy reduction (floor(2^32 / q) undershoots 2^32 / q by 0.406, so the
+    quotient falls one short only when T mod q < 0.406 q T / 2^32 < 10.6)
+    leaves [0, q + 11): a high byte of at most 13."""
+    lo, hi = -16 * 128 * (Q - 1), 16 * (255 + 127) * (Q - 1)
+    assert lo + FIRST_BIAS >= 0 and hi + FIRST_BIAS < 2 ** 25
+    t = np.concatenate([np.arange(lo, lo + 100000), rng(8).integers(lo, hi + 1, 2_000_000),
+                        np.arange(hi - 100000, hi + 1)]) + FIRST_BIAS
+    y = red_lazy(t)
+    assert y.min() >= 0 and y.max() < Q + 11 and ((y - t) % Q == 0).all()
+    assert (Q + 10) >> 8 == 13
 
 
 def test_output_addresses_are_the_tma_swizzle_layout():
@@ -167,63 +205,6 @@ def test_stage_a_operand_reads_stay_in_its_quarter():
                 assert (64 * (m // 4) * 2 + logical) // 2 == 16 * m + k // 2
         assert start % 16 == 0
 
-
-def model_forward(tiles: np.ndarray, x: np.ndarray):
-    """The forward kernel's arithmetic: stage 1 per coefficient c from the
-    transposed operand (K byte 2m + b = byte b of X[m][c]), stage 2 per block
-    i from the bytes of the int32 stage-1 sums, exact reduction to [0, q)."""
-    n = x.shape[0]
-    X = np.ascontiguousarray(x.astype(np.int16)).reshape(n, 16, 16)   # [p][m][c]
-    S1 = np.zeros((n, 16, 16), dtype=np.int64)                          # [p][i][c]
-    for c in range(16):
-        col = np.ascontiguousarray(X[:, :, c]).view(np.uint8).reshape(n, 32)
-        d = as_u8(col) @ tiles[36].T + as_s8(col) @ tiles[37].T
-        assert np.abs(d).max() < 2 ** 31
-        S1[:, :, c] = d[:, :16] + 128 * d[:, 16:]
-    s32 = S1.astype(np.int32)
-    S2 = np.zeros((n, 16, 16), dtype=np.int64)                          # [p][i][c']
-    for i in range(16):
-        by = s32[:, i, :].copy().view(np.uint8).reshape(n, 64)          # byte j of S[c] at 4c + j
-        d = np.zeros((n, 32), dtype=np.int64)
-        for h in range(2):
-            kb = by[:, 32 * h:32 * h + 32]
-            t = 38 + 4 * i + 2 * h
-            d += as_u8(kb) @ tiles[t].T + as_s8(kb) @ tiles[t + 1].T
-        assert np.abs(d).max() < 2 ** 31
-        S2[:, i] = d[:, :16] + 128 * d[:, 16:]
-    quot = (S2 * M40 + Q * 65536 * M40) >> 40
-    r = (S2 - quot * Q) & 0xFFFF
-    return r.astype(np.int16).reshape(n, 256), S1, S2
-
-
-def test_forward_tables_hold_the_stage_matrices(tk):
-    tiles = decode(tk.get_table(8))
-    m1 = tk.get_table(0).astype(np.int64)       # [i][m]
-    m2 = tk.get_table(1).astype(np.int64)       # [block][out][in]
-
-    def limbs(v):
-        return np.concatenate([v & 127, v >> 7])
-    assert (tiles[36][:, 1::2] == 0).all() and (tiles[37][:, 0::2] == 0).all()
-    assert (tiles[36][:, 0::2] == limbs(m1)).all()
-    assert (tiles[37][:, 1::2] == limbs(256 * m1 % Q)).all()
-    for i in range(16):
-        for h in range(2):
-            for cc in range(8):
-                for j in range(4):
-                    col = m2[i][:, 8 * h + cc] * pow(256, j, Q) % Q
-                    u, s = tiles[38 + 4 * i + 2 * h][:, 4 * cc + j], tiles[39 + 4 * i + 2 * h][:, 4 * cc + j]
-                    assert (u == (limbs(col) if j < 3 else 0)).all()
-                    assert (s == (limbs(col) if j == 3 else 0)).all()
-
-
-def test_forward_model_matches_the_oracle_and_bounds_hold(tk, oracle):
-    tiles = decode(tk.get_table(8))
-    x = inputs()
-    out, S1, S2 = model_forward(tiles, x)
-    assert S1.min() >= -(2 ** 24) and S1.max() < 2 ** 25
-    assert S2.min() >= -(2 ** 16) and S2.max() < 2 ** 26
-    assert out.min() >= 0 and out.max() < Q
-    assert (out == canon(oracle.ntt(canon(x).astype(np.int16)))).all()
 
 
 def test_forward_transposition_layout():
