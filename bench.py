@@ -442,8 +442,9 @@ def run_ours(args):
 
 def run_sweep(args):
     """Batch-size sweep: for every power of two up to 2^sweep-max, forward,
-    inverse and round-trip throughput with the autotuned variant, as JSON lines
-    (one per size) in --sweep-out; the summary line goes to stdout."""
+    inverse and round-trip throughput with the autotuned variant, and every
+    variant's time per launch in each direction (mma.sync 0-3, tcgen05 4), as
+    JSON lines (one per size) in --sweep-out; the summary line goes to stdout."""
     import torch
 
     import tensorkyber_b200 as tk
@@ -480,9 +481,28 @@ def run_sweep(args):
                 e1.record(stream)
                 torch.cuda.synchronize()
                 res[name] = e0.elapsed_time(e1) * 1e3 / K   # us per step
+            # every variant in each direction at this size (the autotuner's
+            # candidates: mma.sync shapes 0-3, tcgen05 4), K launches each
+            per_variant = {}
+            for dname, d, f in (("fwd", tk.FORWARD, tk.ntt), ("inv", tk.INVERSE, tk.invntt)):
+                per_variant[dname] = {}
+                for v in range(tk.variant_count()):
+                    tk.set_variant(d, v)
+                    for k in range(3):
+                        f(batches[k % nb], stream=stream)
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    for k in range(K):
+                        f(batches[k % nb], stream=stream)
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    per_variant[dname][str(v)] = e0.elapsed_time(e1) * 1e3 / K
+                tk.set_variant(d, -1)
             row = {
                 "npoly": n,
                 "fwd_us": res["fwd"], "inv_us": res["inv"], "roundtrip_us": res["roundtrip"],
+                "variant_us": per_variant,
                 "polys_per_s": n / (res["roundtrip"] * 1e-6),
                 "hbm_frac": (2 * n * 1024 / (res["roundtrip"] * 1e-6)) / (peak * 1e9),
                 "l2_resident": nb * n * 512 < (126 << 20),
