@@ -277,7 +277,7 @@ int tk_abi_version(void);
  *      kernels upload them
  *   7: the tiled matrix-vector kernel's inverse fragment tables (layout of
  *      5), computing 2^-16 * invntt
- *   8: the tcgen05 kernels' 51 int8 B-operand tiles of 1 KiB (tcgen05 K-major
+ *   8: the tcgen05 kernels' 68 int8 B-operand tiles of 1 KiB (tcgen05 K-major
  *      layout; see tensorkyber_b200/csrc/tk_tables.h)
  * Copies min(bytes, size) bytes to out and returns the table size in bytes,
  * or -TK_ERR_INVALID_VALUE.  Counterpart of setup_tc_matrices

@@ -173,7 +173,7 @@ def get_table(which: int) -> np.ndarray:
     int16 residues; 4 / 5 the forward / inverse fragment tables as raw uint32;
     6 the basemul pair constants as int32[128]; 7 the tiled matrix-vector
     kernel's inverse fragment tables (2^-16 * invntt) as raw uint32; 8 the
-    tcgen05 kernels' 51 int8 B-operand tiles of 1 KiB, raw (view as uint8)."""
+    tcgen05 kernels' 68 int8 B-operand tiles of 1 KiB, raw (view as uint8)."""
     L = lib()
     size = L.tk_get_table(which, None, 0)
     if size < 0:

@@ -269,13 +269,18 @@ void build_tc5_tables(const Matrices& M, uint8_t* out) {
             if (b == 0) put(2 * m, o + 16 * g, 2 * j, limb(M.ma[m][o][j], g));
             else put(2 * m + 1, o + 16 * g, 2 * j + 1, limb(byte_weighted(M.ma[m][o][j], 1), g));
           }
-          // inverse stage B: input block j, byte b
-          put(32, o + 16 * g, 2 * j + b, limb(byte_weighted(M.minv[o][j], b), g));
           // forward stage 1: input block j, byte b (unsigned low / signed high)
-          put(33 + b, o + 16 * g, 2 * j + b, limb(byte_weighted(M.m1[o][j], b), g));
-          // forward stage 2, block i: input coefficient j, byte b
+          put(34 + b, o + 16 * g, 2 * j + b, limb(byte_weighted(M.m1[o][j], b), g));
+        }
+  // second stages: four bytes of an int32 sum per input, two K steps of 8
+  for (int o = 0; o < 16; o++)
+    for (int g = 0; g < 2; g++)
+      for (int j = 0; j < 16; j++)
+        for (int t = 0; t < 4; t++) {
+          const int h = j >> 3, k = 4 * (j & 7) + t;
+          put(32 + h, o + 16 * g, k, limb(byte_weighted(M.minv[o][j], t), g));
           for (int i = 0; i < 16; i++)
-            put(35 + i, o + 16 * g, 2 * j + b, limb(byte_weighted(M.m2[i][o][j], b), g));
+            put(36 + 2 * i + h, o + 16 * g, k, limb(byte_weighted(M.m2[i][o][j], t), g));
         }
 }
 

@@ -133,19 +133,20 @@ void scale_inverse(Matrices* M, int64_t f);
 //                    the low bytes, constant MA[m][out][c']; t = 1 (signed
 //                    data): the high bytes, constant 256 MA[m][out][c'] mod
 //                    q; the other byte's rows are zero.
-//   tile 32          inverse stage B (Minv): K byte k = 2 m + b, byte b of
-//                    the (non-negative, below 2^12) stage-A value of block m;
-//                    constant Minv[out][m] 256^b mod q.
-//   tile 33 + t      forward stage 1 (M1): K byte k = 2 m + b, byte b of the
+//   tile 32 + h      inverse stage B (Minv), K step h: K byte k = 4 (m - 8h)
+//                    + j, byte j of the non-negative (below 2^25) int32
+//                    stage-A sum of block m; constant Minv[out][m] 256^j mod q.
+//   tile 34 + t      forward stage 1 (M1): K byte k = 2 m + b, byte b of the
 //                    block-m coefficient; t = 0: low bytes, constant
 //                    M1[out][m]; t = 1: high bytes, 256 M1[out][m] mod q.
-//   tile 35 + i      forward stage 2 (M2 of block i): K byte k = 2 c + b,
-//                    byte b of the (non-negative, below 2^12) stage-1 value
-//                    of coefficient c; constant M2[i][out][c] 256^b mod q.
-// The inverse uses tiles 0-32, the forward tiles 33-50.
+//   tile 36 + 2i + h forward stage 2 (M2 of block i), K step h: K byte k =
+//                    4 (c - 8h) + j, byte j of the non-negative (below 2^25)
+//                    int32 stage-1 sum of coefficient c; constant
+//                    M2[i][out][c] 256^j mod q.
+// The inverse uses tiles 0-33, the forward tiles 34-67.
 constexpr int kTc5TileBytes = 1024;
-constexpr int kTc5InvTiles = 33;
-constexpr int kTc5FwdTiles = 18;
+constexpr int kTc5InvTiles = 34;
+constexpr int kTc5FwdTiles = 34;
 constexpr int kTc5Tiles = kTc5InvTiles + kTc5FwdTiles;
 constexpr int kTc5TableBytes = kTc5Tiles * kTc5TileBytes;
 inline int tc5_tile_offset(int n, int k) {

@@ -23,12 +23,13 @@
 //     constants on the low bytes' K rows, one with signed data and constants
 //     256 C mod q on the high bytes' K rows; the other rows of each constant
 //     tile are zero.
-//   * The first stage's sums S = D_lo + 128 D_hi get one lazy reduction to
-//     [0, q + 11) and go back to tensor memory packed two to a 32-bit column,
-//     transposed: output n's second-stage operand is the 8 columns 8 n .. 8 n
-//     + 7, read by tcgen05.mma straight from tensor memory, one unsigned MMA
-//     per coefficient (inverse) or block (forward).
-//   * The second stage's sums (below 2^24) get one exact reduction (centred
+//   * The first stage's sums S = D_lo + 128 D_hi are never reduced: S + 2048 q
+//     (non-negative, below 2^25) goes back to tensor memory as int32,
+//     transposed -- output n's second-stage operand is the 16 columns 16 n ..
+//     16 n + 15, read by tcgen05.mma straight from tensor memory as 64
+//     unsigned bytes whose constants carry 256^j mod q, two MMAs per
+//     coefficient (inverse) or block (forward).
+//   * The second stage's sums (below 2^26) get one exact reduction (centred
 //     for the inverse, [0, q) for the forward), are packed to int16 and
 //     written in the TMA layout over the tile's own input slot (its MMAs have
 //     finished), and TMA stores the tile.
@@ -38,10 +39,10 @@
 // tensor-memory allocation); warps 0-7 move data between tensor memory,
 // registers and shared memory, warps w and w + 4 sharing tensor-memory lanes
 // 32 (w % 4) .. + 31 (polynomials) and splitting the columns.  Tensor memory
-// (512 columns): 0-127 the packed first-stage values, 256-383 and 384-511 two
+// (512 columns): 0-255 the first stage's sums, 256-383 and 384-511 two
 // accumulator buffers of four 32-column MMA results each.  Per tile the MMA
-// thread issues 8 chunks of four MMA results (first stage: 8 MMAs each;
-// second stage: 4 each) into the buffers in turn; warps 0-3 take buffer 0,
+// thread issues 8 chunks of four MMA results (8 MMAs each) into the buffers
+// in turn; warps 0-3 take buffer 0,
 // warps 4-7 buffer 1.  Two input slots of 64 KiB: the load of tile k + 2 goes
 // into tile k's slot once tile k's output (written over its input) has been
 // read out by the store.  Every mbarrier wait gives up after 2 s (status bit
@@ -97,9 +98,8 @@ constexpr uint32_t kIdescS8 = kIdescU8 | (1u << 7) | (1u << 10);
 constexpr uint64_t kWaitNs = 2000000000ull;
 // The first stage's sums S (in [-16 * 128 (q-1), 16 * 382 (q-1)]: unsigned
 // low bytes and signed high bytes against constants below q) plus this
-// multiple of q are non-negative and below 2^25, where red_lazy leaves
-// [0, q + 11) (floor(2^32 / q) is 0.406 below 2^32 / q: the quotient is one
-// short only when T mod q < 0.406 q T / 2^32 < 10.6), high byte <= 13.
+// multiple of q are non-negative and below 2^25: bytes 0-2 and a top byte of
+// 0 or 1, all unsigned for the second stage.
 constexpr uint32_t kFirstBias = 2048u * 3329u;
 
 __device__ __align__(128) uint8_t g_tc5_tables[kTc5TableBytes];
@@ -153,8 +153,8 @@ __device__ __forceinline__ uint32_t sw128_chunk(uint32_t slot, uint32_t p, uint3
 // apart).  Warp w reads coefficients 8 (w / 4) .. + 7 of every block of its
 // rows, the 8 warps meet on an mbarrier (bounded wait), then every warp writes
 // its c-tiles over the rows.  Stage 1 runs per c-tile in chunks of c-tiles
-// {0-3}, {4-7}, ..., stage 2 per block i from tensor-memory columns 8 i ..
-// 8 i + 7 against the block's own constant tile, chunks of blocks {0-3},
+// {0-3}, {4-7}, ..., stage 2 per block i from tensor-memory columns 16 i ..
+// 16 i + 15 against the block's own constant tiles, chunks of blocks {0-3},
 // {4-7}, ...; its rows (two 16-byte chunks per block) go to the slot in the
 // TMA layout.
 template <bool kInverse>
@@ -284,8 +284,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
               tc_mma_ss(d, a, tile_desc(2 * idx + 1), kIdescS8, 1);
             } else {
               const uint64_t a = smem_desc(slot_addr(s) + 4096u * idx, 128, 256, kLayoutNone);
-              tc_mma_ss(d, a, tile_desc(33), kIdescU8, 0);
-              tc_mma_ss(d, a, tile_desc(34), kIdescS8, 1);
+              tc_mma_ss(d, a, tile_desc(34), kIdescU8, 0);
+              tc_mma_ss(d, a, tile_desc(35), kIdescS8, 1);
             }
           }
           tc_commit(d_full(b));
@@ -306,8 +306,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
           for (int u = 0; u < 4; u++) {
             const int idx = first + u;
             const uint32_t d = tmem + kColD0 + 128u * b + 32u * u;
-            tc_mma_ts(d, tmem + kColY + 8u * idx, tile_desc(kInverse ? 32 : 35 + idx), kIdescU8,
-                      0);
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+              tc_mma_ts(d, tmem + kColY + 16u * idx + 8u * h,
+                        tile_desc(kInverse ? 32 + h : 36 + 2 * idx + h), kIdescU8, h);
           }
           tc_commit(d_full(b));
           use[b]++;
@@ -372,10 +374,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
         __syncwarp();
         if (lane == 0) mbar_arrive(x_ready);
       }
-      // first stage: S = D_lo + 128 D_hi, lazily reduced to [0, q + 11), packed
-      // in pairs of consecutive MMA results (idx 4j + u): tensor-memory column
-      // 8 n + 2 j + u / 2 of output n holds results 4j + u, 4j + u + 1 (the
-      // second stage's K bytes 4 (2j + u/2) .. + 3), chunks j = half, half + 2
+      // first stage: S = D_lo + 128 D_hi + 2048 q (non-negative, below 2^25)
+      // as int32 to tensor memory column 16 n + idx (output n of the MMA,
+      // idx = 4j + u its position among the tile's first-stage MMAs), the
+      // second stage's K bytes 4 (idx % 8) .. + 3 of step idx / 8; chunks
+      // j = half, half + 2
 #pragma unroll 1
       for (int jj = 0; jj < 2; jj++) {
         const int j = half + 2 * jj;
@@ -389,13 +392,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
         tc_wait_ld();
         give_back();
 #pragma unroll
-        for (int n = 0; n < 16; n++) {
-          const uint32_t v0 = red_lazy(r0[n] + (r0[16 + n] << 7) + kFirstBias);
-          const uint32_t v1 = red_lazy(r0[32 + n] + (r0[48 + n] << 7) + kFirstBias);
-          const uint32_t v2 = red_lazy(r1[n] + (r1[16 + n] << 7) + kFirstBias);
-          const uint32_t v3 = red_lazy(r1[32 + n] + (r1[48 + n] << 7) + kFirstBias);
-          tc_st2(ycol + 8u * n + 2u * j, pack2(v0, v1), pack2(v2, v3));
-        }
+        for (int n = 0; n < 16; n++)
+          tc_st4(ycol + 16u * n + 4u * j, r0[n] + (r0[16 + n] << 7) + kFirstBias,
+                 r0[32 + n] + (r0[48 + n] << 7) + kFirstBias,
+                 r1[n] + (r1[16 + n] << 7) + kFirstBias, r1[32 + n] + (r1[48 + n] << 7) + kFirstBias);
       }
       if (!ok) break;
       tc_wait_st();

@@ -95,7 +95,7 @@ def test_get_table_sizes(tk):
     assert L.tk_get_table(1, None, 0) == 16 * 16 * 16 * 2
     assert L.tk_get_table(6, None, 0) == 128 * 4
     assert L.tk_get_table(7, None, 0) == L.tk_get_table(5, None, 0)
-    assert L.tk_get_table(8, None, 0) == 51 * 1024            # the tcgen05 kernels' tiles
+    assert L.tk_get_table(8, None, 0) == 68 * 1024            # the tcgen05 kernels' tiles
     assert L.tk_get_table(9, None, 0) < 0
     assert L.tk_get_table(-1, None, 0) < 0
     small = (ctypes.c_uint8 * 4)()

@@ -4,9 +4,9 @@ The library's own B-operand tiles (table 8) are decoded from the tcgen05
 K-major layout and pushed through the kernels' integer steps with numpy: the
 first stage as a pair of MMAs per block or coefficient (unsigned data against
 the low-byte constants, signed data against the high-byte constants) into one
-int32 accumulator per constant limb, the recombination S = D_lo + 128 D_hi, a
-lazy reduction of S + 2048 q to [0, q + 11), the second stage as one unsigned
-MMA over the two bytes of those values, and the exact (forward) or centred
+int32 accumulator per constant limb, the recombination S = D_lo + 128 D_hi
+plus 2048 q (non-negative, below 2^25), the second stage as two unsigned MMAs
+over the four bytes of those sums, and the exact (forward) or centred
 (inverse) reduction.  Every coefficient must agree with the oracle mod q, the
 intermediate bounds the kernels rely on must hold, and the shared-memory
 addresses they read and write must be the TMA 128-byte-swizzle layout of the
@@ -17,9 +17,8 @@ from conftest import rng
 from py_oracle import Q, canon
 
 TILE_BYTES = 1024
-NTILES = 51           # 0-32 the inverse's, 33-50 the forward's
+NTILES = 68           # 0-33 the inverse's, 34-67 the forward's
 FIRST_BIAS = 2048 * Q
-BAR_LAZY = 1290167    # floor(2^32 / q)
 BAR_EXACT = 82570715  # ceil(2^38 / q)
 
 
@@ -30,7 +29,7 @@ def tile_offset(n, k):
 def decode(raw: np.ndarray) -> np.ndarray:
     """The tiles of B[n][k] (n = out + 16 limb, k = K byte), each read back from
     the K-major core-matrix layout; the signed-data tiles (1, 3, .., 31 and
-    34) as signed bytes, the others unsigned."""
+    35) as signed bytes, the others unsigned."""
     raw = raw.view(np.uint8)
     assert raw.size == NTILES * TILE_BYTES
     off = np.array([[tile_offset(n, k) for k in range(32)] for n in range(32)])
@@ -38,7 +37,7 @@ def decode(raw: np.ndarray) -> np.ndarray:
     tiles = np.zeros((NTILES, 32, 32), dtype=np.int64)
     for t in range(NTILES):
         b = raw[t * TILE_BYTES:(t + 1) * TILE_BYTES][off]
-        signed = (t < 32 and t & 1) or t == 34
+        signed = (t < 32 and t & 1) or t == 35
         tiles[t] = b.view(np.int8) if signed else b
     return tiles
 
@@ -51,28 +50,21 @@ def as_s8(a):
     return a.astype(np.uint8).view(np.int8).astype(np.int64)
 
 
-def red_lazy(t):
-    assert t.min() >= 0 and t.max() < 2 ** 25
-    return t - ((t * BAR_LAZY) >> 32) * Q
-
-
-def first_stage_values(d):
-    """[n][32] accumulators -> lazily reduced values [n][16] in [0, q + 11)."""
+def first_stage_sums(d):
+    """[n][32] accumulators -> S + 2048 q [n][16], non-negative, below 2^25."""
     assert np.abs(d).max() < 2 ** 31
-    s = d[:, :16] + 128 * d[:, 16:]
-    assert s.min() >= -(2 ** 24) and s.max() < 2 ** 25
-    y = red_lazy(s + FIRST_BIAS)
-    assert y.min() >= 0 and y.max() < Q + 11
-    return y
+    s = d[:, :16] + 128 * d[:, 16:] + FIRST_BIAS
+    assert s.min() >= 0 and s.max() < 2 ** 25
+    return s
 
 
-def second_stage(y_cols, tile):
-    """y_cols[n][16] values (K byte 2 v + b = byte b of value v) against one
-    unsigned tile -> S = D_lo + 128 D_hi [n][16], non-negative, < 2^24."""
-    by = np.stack([y_cols & 255, y_cols >> 8], axis=2).reshape(y_cols.shape[0], 32)
-    d = by @ tile.T
+def second_stage(sums, tiles):
+    """sums[n][16] (K byte 4 (v % 8) + j of step v / 8 = byte j of sum v)
+    against two unsigned tiles -> S = D_lo + 128 D_hi [n][16], below 2^26."""
+    by = sums.astype(np.int32).view(np.uint8).reshape(sums.shape[0], 64).astype(np.int64)
+    d = by[:, :32] @ tiles[0].T + by[:, 32:] @ tiles[1].T
     s = d[:, :16] + 128 * d[:, 16:]
-    assert s.min() >= 0 and s.max() < 2 ** 24
+    assert s.min() >= 0 and s.max() < 2 ** 26
     return s
 
 
@@ -82,10 +74,10 @@ def model_inverse(tiles: np.ndarray, x: np.ndarray):
     Y = np.zeros((n, 16, 16), dtype=np.int64)           # [poly][m][c]
     for m in range(16):
         d = as_u8(raw[:, m]) @ tiles[2 * m].T + as_s8(raw[:, m]) @ tiles[2 * m + 1].T
-        Y[:, m] = first_stage_values(d)
+        Y[:, m] = first_stage_sums(d)
     out = np.zeros((n, 16, 16), dtype=np.int64)         # [poly][i][c]
     for c in range(16):
-        s = second_stage(Y[:, :, c], tiles[32])
+        s = second_stage(np.ascontiguousarray(Y[:, :, c]), tiles[32:34])
         quot = ((s * BAR_EXACT + 1664 * BAR_EXACT) >> 38)   # red_centred
         out[:, :, c] = s - quot * Q
     assert out.min() >= -(Q // 2) and out.max() <= Q // 2
@@ -98,11 +90,11 @@ def model_forward(tiles: np.ndarray, x: np.ndarray):
     Y = np.zeros((n, 16, 16), dtype=np.int64)                         # [p][i][c]
     for c in range(16):
         col = np.ascontiguousarray(X[:, :, c]).view(np.uint8).reshape(n, 32)
-        d = as_u8(col) @ tiles[33].T + as_s8(col) @ tiles[34].T
-        Y[:, :, c] = first_stage_values(d)
+        d = as_u8(col) @ tiles[34].T + as_s8(col) @ tiles[35].T
+        Y[:, :, c] = first_stage_sums(d)
     out = np.zeros((n, 16, 16), dtype=np.int64)                       # [p][i][c']
     for i in range(16):
-        s = second_stage(Y[:, i, :], tiles[35 + i])
+        s = second_stage(np.ascontiguousarray(Y[:, i, :]), tiles[36 + 2 * i:38 + 2 * i])
         out[:, i] = s - ((s * BAR_EXACT) >> 38) * Q                   # red_exact
     assert out.min() >= 0 and out.max() < Q
     return out.reshape(n, 256).astype(np.int16)
@@ -122,8 +114,8 @@ def limbs(v):
 
 
 def test_tables_hold_the_stage_matrices(tk):
-    """Decoded tiles: limbs of the stage constants (times 256 on the high
-    bytes' K rows) and zeros on the rows the other MMA kind covers."""
+    """Decoded tiles: limbs of the stage constants (times 256^j on byte j's K
+    rows) and zeros on the rows the other MMA kind covers."""
     tiles = decode(tk.get_table(8))
     m1 = tk.get_table(0).astype(np.int64)       # [i][m]
     m2 = tk.get_table(1).astype(np.int64)       # [block][out][in]
@@ -133,14 +125,17 @@ def test_tables_hold_the_stage_matrices(tk):
         assert (tiles[2 * m][:, 1::2] == 0).all() and (tiles[2 * m + 1][:, 0::2] == 0).all()
         assert (tiles[2 * m][:, 0::2] == limbs(ma[m])).all()
         assert (tiles[2 * m + 1][:, 1::2] == limbs(256 * ma[m] % Q)).all()
-    assert (tiles[32][:, 0::2] == limbs(minv)).all()
-    assert (tiles[32][:, 1::2] == limbs(256 * minv % Q)).all()
-    assert (tiles[33][:, 1::2] == 0).all() and (tiles[34][:, 0::2] == 0).all()
-    assert (tiles[33][:, 0::2] == limbs(m1)).all()
-    assert (tiles[34][:, 1::2] == limbs(256 * m1 % Q)).all()
-    for i in range(16):
-        assert (tiles[35 + i][:, 0::2] == limbs(m2[i])).all()
-        assert (tiles[35 + i][:, 1::2] == limbs(256 * m2[i] % Q)).all()
+    assert (tiles[34][:, 1::2] == 0).all() and (tiles[35][:, 0::2] == 0).all()
+    assert (tiles[34][:, 0::2] == limbs(m1)).all()
+    assert (tiles[35][:, 1::2] == limbs(256 * m1 % Q)).all()
+    for h in range(2):
+        for v in range(8):
+            for j in range(4):
+                w = pow(256, j, Q)
+                assert (tiles[32 + h][:, 4 * v + j] == limbs(minv[:, 8 * h + v] * w % Q)).all()
+                for i in range(16):
+                    assert (tiles[36 + 2 * i + h][:, 4 * v + j] ==
+                            limbs(m2[i][:, 8 * h + v] * w % Q)).all()
 
 
 def test_inverse_model_matches_the_oracle(tk, oracle):
@@ -156,17 +151,11 @@ def test_forward_model_matches_the_oracle(tk, oracle):
 def test_first_stage_bias_covers_the_sum_range():
     """The first stage's sums lie in [-16 * 128 (q-1), 16 * 382 (q-1)]
     (16 inputs of unsigned low and signed high bytes against constants below
-    q); adding 2048 q makes them non-negative and keeps them below 2^25, where
-    the lazy reduction (floor(2^32 / q) undershoots 2^32 / q by 0.406, so the
-    quotient falls one short only when T mod q < 0.406 q T / 2^32 < 10.6)
-    leaves [0, q + 11): a high byte of at most 13."""
+    q); adding 2048 q makes them non-negative and keeps them below 2^25, so
+    their four bytes are unsigned (the top one 0 or 1)."""
     lo, hi = -16 * 128 * (Q - 1), 16 * (255 + 127) * (Q - 1)
     assert lo + FIRST_BIAS >= 0 and hi + FIRST_BIAS < 2 ** 25
-    t = np.concatenate([np.arange(lo, lo + 100000), rng(8).integers(lo, hi + 1, 2_000_000),
-                        np.arange(hi - 100000, hi + 1)]) + FIRST_BIAS
-    y = red_lazy(t)
-    assert y.min() >= 0 and y.max() < Q + 11 and ((y - t) % Q == 0).all()
-    assert (Q + 10) >> 8 == 13
+    assert (FIRST_BIAS % Q) == 0
 
 
 def test_output_addresses_are_the_tma_swizzle_layout():
