@@ -87,6 +87,10 @@ def parse():
     p.add_argument("--serve-zero-copy", action="store_true")
     p.add_argument("--serve-plain-mode", type=int, default=2,
                    help="matrix-vector mode of the plain per-request path (0, 1, 2 as --matvec-mode)")
+    p.add_argument("--traffic", action="store_true",
+                   help="each direction's launch followed by a read-only pass over 4x the L2, "
+                        "--steps times (for ncu --cache-control none: the pass's DRAM writes "
+                        "are the launch's write-back)")
     return p.parse_args()
 
 
@@ -525,6 +529,50 @@ def run_sweep(args):
     }), flush=True)
 
 
+def run_traffic(args):
+    """DRAM traffic of one launch including its write-back.  The L2 is
+    write-back: part of a launch's output is still dirty in L2 when the launch
+    ends and reaches DRAM later, inside whichever kernel evicts it.  Here every
+    launch is followed by a read-only pass (a sum) over a buffer four times the
+    L2, which evicts every dirty line and writes nothing of its own, so under
+    `ncu --cache-control none` a launch's whole traffic is its own
+    dram__bytes_read.sum + dram__bytes_write.sum plus the pass's
+    dram__bytes_write.sum.  Prints the configuration; the figures come from
+    ncu."""
+    import numpy as np
+    import torch
+
+    import tensorkyber_b200 as tk
+
+    torch.cuda.set_device(0)
+    tk.init(0)
+    apply_variants(tk, args)
+    n = args.npoly
+    gen = np.random.default_rng(1000)
+    data = torch.from_numpy(gen.integers(0, Q, size=(n, 256), dtype=np.int16)).cuda()
+    drain = torch.ones(4 * 126 * 2**20 // 4, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    total = torch.zeros((), dtype=torch.int64, device="cuda")
+    drain.sum()                      # the drain buffer itself clean before the first launch
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        tk.ntt(data, stream=stream)
+        total += drain.sum()
+        tk.invntt(data, stream=stream)
+        total += drain.sum()
+    torch.cuda.synchronize()
+    status = tk.device_status(0)
+    if status:
+        raise RuntimeError(f"kernel status flags {status:#x}")
+    print(json.dumps({
+        "metric": "DRAM traffic per launch incl. write-back (read with ncu)",
+        "npoly": n, "steps": args.steps, "drain_bytes": drain.numel() * 4,
+        "kernel_variant": {"forward": tk.variant_name(tk.get_variant(tk.FORWARD, n)),
+                           "inverse": tk.variant_name(tk.get_variant(tk.INVERSE, n))},
+        "sequence": "ntt, sum(drain), invntt, sum(drain) per step",
+    }), flush=True)
+
+
 def run_forms(args):
     """Forward NTT by input form at --npoly polynomials (default 2^20): int16
     (tk_ntt), small int16 in [-128, 127] (tk_ntt_small, single-limb stage 1),
@@ -847,11 +895,12 @@ def launch_ranks(args) -> int:
 def main():
     args = parse()
     world_env = os.environ.get("WORLD_SIZE")
-    single = args.serve or args.forms or args.matvec or args.sweep
+    single = args.serve or args.forms or args.matvec or args.sweep or args.traffic
     if args.gpus < 1:
         sys.exit("bench.py: --gpus must be at least 1")
     if single and (args.gpus > 1 or (world_env is not None and int(world_env) > 1)):
-        sys.exit("bench.py: --serve, --forms, --matvec and --sweep run on one GPU (--gpus 1)")
+        sys.exit("bench.py: --serve, --forms, --matvec, --sweep and --traffic run on one GPU "
+                 "(--gpus 1)")
     if world_env is None and args.gpus > 1:
         sys.exit(launch_ranks(args))
     if world_env is not None and int(world_env) != args.gpus:
@@ -865,6 +914,8 @@ def main():
         run_matvec(args)
     elif args.sweep:
         run_sweep(args)
+    elif args.traffic:
+        run_traffic(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

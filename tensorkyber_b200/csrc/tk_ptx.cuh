@@ -239,20 +239,21 @@ __device__ __forceinline__ void tc_commit(uint32_t bar) {
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
       : "memory");
 }
-__device__ __forceinline__ void tc_wait_ld() {
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
 __device__ __forceinline__ void tc_wait_st() {
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
-// 64 consecutive 32-bit columns of this thread's lane.
-__device__ __forceinline__ void tc_ld64(uint32_t taddr, uint32_t (&r)[64]) {
+// 64 consecutive 32-bit columns of this thread's lane, waited for in the same
+// statement: tcgen05.ld writes its registers asynchronously, so the values
+// exist only after tcgen05.wait::ld, and a separate wait statement would not
+// stop the compiler from computing with the registers before it.
+__device__ __forceinline__ void tc_ld64_sync(uint32_t taddr, uint32_t (&r)[64]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
       "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
       "%28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, "
       "%45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, "
-      "%62, %63}, [%64];"
+      "%62, %63}, [%64];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
         "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
@@ -264,7 +265,8 @@ __device__ __forceinline__ void tc_ld64(uint32_t taddr, uint32_t (&r)[64]) {
         "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]),
         "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]),
         "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
-      : "r"(taddr));
+      : "r"(taddr)
+      : "memory");
 }
 // 2 consecutive 32-bit columns of this thread's lane.
 __device__ __forceinline__ void tc_st2(uint32_t taddr, uint32_t a, uint32_t b) {

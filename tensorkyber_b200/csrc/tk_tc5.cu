@@ -34,20 +34,21 @@
 //     written in the TMA layout over the tile's own input slot (its MMAs have
 //     finished), and TMA stores the tile.
 //
-// Roles (320 threads, one CTA per SM by shared memory): warp 9 lane 0 issues
-// TMA loads and stores; warp 8 lane 0 issues MMAs (and warp 8 owns the
-// tensor-memory allocation); warps 0-7 move data between tensor memory,
-// registers and shared memory, warps w and w + 4 sharing tensor-memory lanes
-// 32 (w % 4) .. + 31 (polynomials) and splitting the columns.  Tensor memory
-// (512 columns): 0-255 the first stage's sums, 256-383 and 384-511 two
-// accumulator buffers of four 32-column MMA results each.  Per tile the MMA
-// thread issues 8 chunks of four MMA results (8 MMAs each) into the buffers
-// in turn; warps 0-3 take buffer 0,
-// warps 4-7 buffer 1.  Two input slots of 64 KiB: the load of tile k + 2 goes
-// into tile k's slot once tile k's output (written over its input) has been
-// read out by the store.  Every mbarrier wait gives up after 2 s (status bit
-// 0 forward / 1 inverse, as the other kernels); the MMA thread then drains
-// its MMAs and the producer its copies before the CTA frees tensor memory and
+// Roles (576 threads, one CTA per SM by shared memory): warp 17 lane 0
+// issues TMA loads and stores; warp 16 lane 0 issues MMAs (and warp 16 owns
+// the tensor-memory allocation); warps 0-15 move data between tensor memory,
+// registers and shared memory in four groups of four, warp w reaching
+// tensor-memory lanes 32 (w % 4) .. + 31 (polynomials).  Tensor memory (512
+// columns): 0-255 the first stage's sums, 256 + 64 g .. + 63 group g's
+// accumulator buffer (two 32-column MMA results).  Per tile the MMA thread
+// issues 16 chunks of two results, chunk j into buffer j % 4, so the MMAs of
+// one group's chunk run while the other groups read theirs, and the next
+// tile's first stage starts while this tile's second-stage results are still
+// being read.  Three slots of 64 KiB: the load of tile k + 3 goes into tile
+// k's slot once tile k's output (written over its input) has been read out
+// by the store.  Every mbarrier wait gives up after 2 s (status bit 0
+// forward / 1 inverse, as the other kernels); the MMA thread then drains its
+// MMAs and the producer its copies before the CTA frees tensor memory and
 // exits.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -66,15 +67,19 @@ namespace {
 constexpr int kTcTile = 128;                      // polynomials per tile (MMA M)
 constexpr int kTcQuarterBytes = kTcTile * 128;    // one 64-coefficient box: 16 KiB
 constexpr int kTcSlotBytes = 4 * kTcQuarterBytes;  // 64 KiB
-constexpr int kTcEpiWarps = 8;
-constexpr int kTcMmaWarp = 8, kTcTmaWarp = 9;
+constexpr int kTcSlots = 3;
+// epilogue warp groups: group g (warps 4g .. 4g + 3, one per tensor-memory
+// lane quarter) owns accumulator buffer g
+constexpr int kTcGroups = 4;
+constexpr int kTcEpiWarps = 4 * kTcGroups;
+constexpr int kTcMmaWarp = kTcEpiWarps, kTcTmaWarp = kTcEpiWarps + 1;
 constexpr int kTcThreads = 32 * (kTcEpiWarps + 2);
-// dynamic shared memory, from a 1024-byte aligned base (the swizzle atom):
-// two 64 KiB tile slots, this direction's constant tiles, the mbarriers
-// (in_full[2], out_ready[2], d_full[2], d_empty[2], y_full, x_ready, consts,
-// drain, x_read) and the tensor-memory base address
-constexpr int kOffTables = 2 * kTcSlotBytes;
-constexpr int kNumBars = 13;
+// dynamic shared memory (its base is 1024-byte aligned, the swizzle atom;
+// the kernel checks): three 64 KiB tile slots, this direction's constant
+// tiles, the mbarriers (in_full[3], out_ready[3], d_full[4], d_empty[4],
+// y_full, x_ready, x_read, consts, drain) and the tensor-memory base address
+constexpr int kOffTables = kTcSlots * kTcSlotBytes;
+constexpr int kNumBars = 2 * kTcSlots + 2 * kTcGroups + 5;
 template <bool kInverse>
 struct Tc5Layout {
   static constexpr int kTiles = kInverse ? kTc5InvTiles : kTc5FwdTiles;
@@ -82,14 +87,14 @@ struct Tc5Layout {
   static constexpr int kTableBytes = kTiles * kTc5TileBytes;
   static constexpr int kOffBars = kOffTables + kTableBytes;
   static constexpr int kOffTmemSlot = kOffBars + 8 * kNumBars;
-  static constexpr int kSmemBytes = kOffTmemSlot + 8 + 1024;  // + slack to align the base
+  static constexpr int kSmemBytes = kOffTmemSlot + 8;
   static_assert(2 * kSmemBytes > 228 * 1024, "one CTA per SM: it owns all tensor memory");
   static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
 };
 // tensor memory
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kColY = 0;
-constexpr uint32_t kColD0 = 256;  // accumulator buffer b at kColD0 + 128 b
+constexpr uint32_t kColD0 = 256;  // group g's accumulator buffer at kColD0 + 64 g
 // instruction descriptors of kind::i8: D format s32 (bits 4-5 = 2), A / B
 // format (bits 7-9 / 10-12: 0 unsigned, 1 signed), K-major A and B, N >> 3
 // (bits 17-22) = 4, M >> 4 (bits 24-28) = 8: M = 128, N = 32, K = 32.
@@ -113,8 +118,8 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 }
 constexpr uint32_t kLayoutNone = 0, kLayoutSw128 = 2;
 
-__device__ __forceinline__ void st_shared_v2(uint32_t addr, uint32_t a, uint32_t b) {
-  asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(addr), "r"(a), "r"(b) : "memory");
+__device__ __forceinline__ void st_shared_u32(uint32_t addr, uint32_t a) {
+  asm volatile("st.shared.u32 [%0], %1;" ::"r"(addr), "r"(a) : "memory");
 }
 __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c,
                                              uint32_t d) {
@@ -129,6 +134,9 @@ __device__ __forceinline__ uint4 ld_shared_v4(uint32_t addr) {
                : "r"(addr)
                : "memory");
   return v;
+}
+__device__ __forceinline__ uint32_t word_of(const uint4& v, int i) {
+  return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
 }
 
 struct Tc5Params {
@@ -146,24 +154,35 @@ __device__ __forceinline__ uint32_t sw128_chunk(uint32_t slot, uint32_t p, uint3
   return slot + (k >> 3) * kTcQuarterBytes + p * 128u + (((k & 7u) ^ (p & 7u)) << 4);
 }
 
+// Per tile the MMA thread issues 16 chunks of two 32-column MMA results:
+// first stage a = 0..7 (results 2a, 2a + 1: inverse blocks, forward
+// coefficients), second stage b = 0..7 (results n = 4 (b % 4) + 2 (b / 4) and
+// n + 1: inverse coefficients, forward blocks); chunk a or b goes to buffer
+// (and warp group) a % 4 or b % 4, so group g reads first-stage chunks g, g+4
+// and the second-stage results 4g .. 4g + 3.  The MMAs of one chunk can run
+// while the other groups read theirs; the second stage waits for the whole
+// first stage in tensor memory (y_full), the next tile's first stage only
+// for its buffers.
+//
 // The forward's transposition: for coefficient c (c-tile c, 4 KiB at 4096 c
 // of the slot), row p's 32 K bytes are the blocks' values X[m][c] in block
 // order (K byte 2m + b), K-major without swizzle (8-row core matrices of
 // 16-byte rows, the two K halves 128 bytes apart, 8-row groups 256 bytes
-// apart).  Warp w reads coefficients 8 (w / 4) .. + 7 of every block of its
-// rows, the 8 warps meet on an mbarrier (bounded wait), then every warp writes
-// its c-tiles over the rows.  Stage 1 runs per c-tile in chunks of c-tiles
-// {0-3}, {4-7}, ..., stage 2 per block i from tensor-memory columns 16 i ..
-// 16 i + 15 against the block's own constant tiles, chunks of blocks {0-3},
-// {4-7}, ...; its rows (two 16-byte chunks per block) go to the slot in the
-// TMA layout.
+// apart).  The four warps of a lane quarter split each row: group g reads
+// coefficients 8 (g % 2) .. + 7 of blocks 8 (g / 2) .. + 7 (eight 16-byte
+// chunks), the 16 warps meet on an mbarrier (bounded wait), then every warp
+// writes its half-K rows of c-tiles 8 (g % 2) .. + 7.  Tile k + 1 is
+// transposed between tile k's two stages, while the second stage's first
+// MMAs run.
 template <bool kInverse>
 __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ Tc5Params P) {
   using L = Tc5Layout<kInverse>;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  const uint32_t raw = smem_u32(smem_raw);
-  const uint32_t base = (raw + 1023u) & ~1023u;
-  uint8_t* const basep = smem_raw + (base - raw);
+  const uint32_t base = smem_u32(smem_raw);
+  if (base & 1023u) {  // the swizzled slots need the 1024-byte atom alignment
+    if (threadIdx.x == 0) atomicOr(P.status, kInverse ? 2u : 1u);
+    return;
+  }
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int G = (int)gridDim.x;
   const int t_begin = (int)((long long)blockIdx.x * P.ntiles / G);
@@ -173,25 +192,28 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
   const uint32_t tables = base + kOffTables;
   const uint32_t bars = base + L::kOffBars;
   auto in_full = [&](int s) { return bars + 8u * s; };
-  auto out_ready = [&](int s) { return bars + 16u + 8u * s; };
-  auto d_full = [&](int b) { return bars + 32u + 8u * b; };
-  auto d_empty = [&](int b) { return bars + 48u + 8u * b; };
-  const uint32_t y_full = bars + 64u, x_ready = bars + 72u, consts = bars + 80u,
-                 drain = bars + 88u, x_read = bars + 96u;
+  auto out_ready = [&](int s) { return bars + 8u * (kTcSlots + s); };
+  auto d_full = [&](int g) { return bars + 8u * (2 * kTcSlots + g); };
+  auto d_empty = [&](int g) { return bars + 8u * (2 * kTcSlots + kTcGroups + g); };
+  constexpr uint32_t kB = 8u * (2 * kTcSlots + 2 * kTcGroups);
+  const uint32_t y_full = bars + kB, x_ready = bars + kB + 8u, x_read = bars + kB + 16u,
+                 consts = bars + kB + 24u, drain = bars + kB + 32u;
   auto slot_addr = [&](int s) { return base + (uint32_t)s * kTcSlotBytes; };
 
   if (tid == 0) {
-    for (int s = 0; s < 2; s++) {
+    for (int s = 0; s < kTcSlots; s++) {
       mbar_init(in_full(s), 1);
       mbar_init(out_ready(s), kTcEpiWarps);
-      mbar_init(d_full(s), 1);
-      mbar_init(d_empty(s), 4);
+    }
+    for (int g = 0; g < kTcGroups; g++) {
+      mbar_init(d_full(g), 1);
+      mbar_init(d_empty(g), 4);
     }
     mbar_init(y_full, kTcEpiWarps);
     mbar_init(x_ready, kTcEpiWarps);
+    mbar_init(x_read, kTcEpiWarps);
     mbar_init(consts, 1);
     mbar_init(drain, 1);
-    mbar_init(x_read, kTcEpiWarps);
     fence_mbar_init();
   }
   if (warp == kTcMmaWarp) {
@@ -201,7 +223,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
   tc_fence_before();
   __syncthreads();  // the mbarriers are initialised (and fenced) before any use
   tc_fence_after();
-  const uint32_t tmem = *(volatile uint32_t*)(basep + L::kOffTmemSlot);
+  const uint32_t tmem = *(volatile uint32_t*)(smem_raw + L::kOffTmemSlot);
   if (warp == kTcTmaWarp && lane == 0) {  // constant tiles (written once by the host)
     mbar_expect_tx(consts, L::kTableBytes);
     bulk_g2s(tables, P.tables, L::kTableBytes, consts);
@@ -213,19 +235,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
   bool ok = true;
   if (warp == kTcTmaWarp) {
     if (lane == 0) {
-      // ---- producer: loads two tiles ahead, stores each tile's output ----
-      int last_load[2] = {-1, -1};
-      auto load = [&](int k, int s) {
+      // ---- producer: loads three tiles ahead, stores each tile's output ----
+      int last_load[kTcSlots];
+      for (int s = 0; s < kTcSlots; s++) last_load[s] = -1;
+      auto load = [&](int k) {
+        const int s = k % kTcSlots;
         mbar_expect_tx(in_full(s), kTcSlotBytes);
         const int row = kTcTile * (t_begin + k);
         for (int q = 0; q < 4; q++)
           tma_load_2d(slot_addr(s) + q * kTcQuarterBytes, &P.in, 64 * q, row, in_full(s));
         last_load[s] = k;
       };
-      for (int k = 0; k < 2 && k < nmine; k++) load(k, k);
+      for (int k = 0; k < kTcSlots && k < nmine; k++) load(k);
       for (int k = 0; k < nmine; k++) {
-        const int s = k & 1;
-        if (!mbar_wait_bounded(out_ready(s), (uint32_t)(k >> 1) & 1u, kWaitNs)) {
+        const int s = k % kTcSlots;
+        if (!mbar_wait_bounded(out_ready(s), (uint32_t)(k / kTcSlots) & 1u, kWaitNs)) {
           ok = false;
           break;
         }
@@ -234,85 +258,102 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
           tma_store_2d(&P.out, 64 * q, row, slot_addr(s) + q * kTcQuarterBytes);
         bulk_commit();
         bulk_wait_read<0>();  // the slot may be refilled
-        if (k + 2 < nmine) load(k + 2, s);
+        if (k + kTcSlots < nmine) load(k + kTcSlots);
       }
       bulk_wait_all();
       // after a give-up: let issued loads land before the CTA's memory goes
-      for (int s = 0; s < 2; s++)
+      for (int s = 0; s < kTcSlots; s++)
         if (last_load[s] >= 0)
-          ok &= mbar_wait_bounded(in_full(s), (uint32_t)(last_load[s] >> 1) & 1u, kWaitNs);
+          ok &= mbar_wait_bounded(in_full(s), (uint32_t)(last_load[s] / kTcSlots) & 1u, kWaitNs);
       ok &= mbar_wait_bounded(consts, 0, kWaitNs);
     }
   } else if (warp == kTcMmaWarp) {
-    if (lane == 0 && nmine > 0) {
+    if (lane == 0) {
       // ---- MMA issuer ----
+      // One thread issues every MMA, so its instruction chain per MMA sets
+      // the issue rate: descriptors are built once (a shared-memory
+      // descriptor's low 14 bits are the address / 16, so an operand at
+      // byte offset o is the base descriptor + o / 16; every address here is
+      // below 2^18) and the chunk loops are unrolled, leaving an add and the
+      // MMA per operand pair.
+      const uint64_t b_desc0 = smem_desc(tables, 128, 256, kLayoutNone);
       auto tile_desc = [&](int i) {
-        return smem_desc(tables + (uint32_t)(i - L::kFirstTile) * kTc5TileBytes, 128, 256,
-                         kLayoutNone);
+        return b_desc0 + (uint64_t)((i - L::kFirstTile) * (kTc5TileBytes >> 4));
       };
-      uint32_t use[2] = {0, 0};
-      auto take = [&](int b) {  // the buffer's previous contents were read out
-        if (use[b] > 0 && !mbar_wait_bounded(d_empty(b), (use[b] - 1) & 1u, kWaitNs))
+      const uint64_t a_desc0 = kInverse ? smem_desc(base, 16, 1024, kLayoutSw128)
+                                        : smem_desc(base, 128, 256, kLayoutNone);
+      // buffer g's previous contents were read out: every tile uses each
+      // buffer four times (first-stage chunks g, g + 4, second-stage chunks
+      // g, g + 4), so the use at position pos (0..3) of tile k is use 4k +
+      // pos and waits for the release of use 4k + pos - 1
+      auto take = [&](int g, int k, int pos) {
+        if ((k > 0 || pos > 0) && !mbar_wait_bounded(d_empty(g), (uint32_t)(pos + 1) & 1u, kWaitNs))
           return false;
         tc_fence_after();
         return true;
       };
       ok = mbar_wait_bounded(consts, 0, kWaitNs);
       for (int k = 0; k < nmine && ok; k++) {
-        const int s = k & 1;
+        const int s = k % kTcSlots;
         // inverse: the loaded tile is stage A's operand; forward: wait for
         // the epilogue warps' transposed copy of it
         if (kInverse)
-          ok = mbar_wait_bounded(in_full(s), (uint32_t)(k >> 1) & 1u, kWaitNs);
+          ok = mbar_wait_bounded(in_full(s), (uint32_t)(k / kTcSlots) & 1u, kWaitNs);
         else
           ok = mbar_wait_bounded(x_ready, (uint32_t)k & 1u, kWaitNs);
         if (!ok) break;
         tc_fence_after();
-        // first stage: chunk j = four MMA pairs (inverse: blocks 4j..4j+3 of
-        // input quarter j; forward: c-tiles 4j..4j+3)
-        for (int j = 0; j < 4 && ok; j++) {
-          const int b = j & 1;
-          if (!(ok = take(b))) break;
+        const uint64_t a_slot = a_desc0 + (uint64_t)(s * (kTcSlotBytes >> 4));
+        // first stage: chunk a = results 2a, 2a + 1 (inverse: blocks of input
+        // quarter a / 2; forward: c-tiles), an MMA pair each.  Chunks go out
+        // two at a time, the first MMA of all four results before any second
+        // one: the second accumulates onto the first's result and waits for
+        // it, and the tensor pipe issues in order, so the four independent
+        // first MMAs cover that latency.
 #pragma unroll
-          for (int u = 0; u < 4; u++) {
-            const int idx = 4 * j + u;
-            const uint32_t d = tmem + kColD0 + 128u * b + 32u * u;
-            if (kInverse) {
-              const uint64_t a = smem_desc(slot_addr(s) + j * kTcQuarterBytes + 32 * u, 16, 1024,
-                                           kLayoutSw128);
-              tc_mma_ss(d, a, tile_desc(2 * idx), kIdescU8, 0);
-              tc_mma_ss(d, a, tile_desc(2 * idx + 1), kIdescS8, 1);
-            } else {
-              const uint64_t a = smem_desc(slot_addr(s) + 4096u * idx, 128, 256, kLayoutNone);
-              tc_mma_ss(d, a, tile_desc(34), kIdescU8, 0);
-              tc_mma_ss(d, a, tile_desc(35), kIdescS8, 1);
+        for (int a = 0; a < 8; a += 2) {
+          if (!(ok = take(a & 3, k, a >> 2) && take((a + 1) & 3, k, a >> 2))) break;
+#pragma unroll
+          for (int t = 0; t < 2; t++) {
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+              const int idx = 2 * a + r, g = (a + (r >> 1)) & 3;
+              const uint32_t d = tmem + kColD0 + 64u * g + 32u * (r & 1);
+              if (kInverse) {
+                const uint64_t ad =
+                    a_slot + (uint64_t)(((idx >> 2) * kTcQuarterBytes + 32 * (idx & 3)) >> 4);
+                tc_mma_ss(d, ad, tile_desc(2 * idx + t), t ? kIdescS8 : kIdescU8, t);
+              } else {
+                const uint64_t ad = a_slot + (uint64_t)((4096 * idx) >> 4);
+                tc_mma_ss(d, ad, tile_desc(34 + t), t ? kIdescS8 : kIdescU8, t);
+              }
+            }
+            if (t == 1) {
+              tc_commit(d_full(a & 3));
+              tc_commit(d_full((a + 1) & 3));
             }
           }
-          tc_commit(d_full(b));
-          use[b]++;
         }
         if (!ok) break;
-        // second stage from tensor memory: inverse coefficient sets {0-3},
-        // {8-11}, {4-7}, {12-15}; forward blocks {0-3}, {4-7}, ...
+        // second stage from tensor memory, two K steps per result, in the
+        // same order (chunks b, b + 1: both results' K step 0, then step 1)
         if (!(ok = mbar_wait_bounded(y_full, (uint32_t)k & 1u, kWaitNs))) break;
         tc_fence_after();
-        for (int j = 0; j < 4 && ok; j++) {
-          const int b = j & 1;
-          if (!(ok = take(b))) break;
-          // inverse: coefficient sets {0-3}, {8-11}, {4-7}, {12-15} (buffer 0,
-          // warps 0-3: 0-7; buffer 1, warps 4-7: 8-15); forward: blocks 4j ..
-          const int first = kInverse ? 8 * (j & 1) + 4 * (j >> 1) : 4 * j;
 #pragma unroll
-          for (int u = 0; u < 4; u++) {
-            const int idx = first + u;
-            const uint32_t d = tmem + kColD0 + 128u * b + 32u * u;
+        for (int b = 0; b < 8; b += 2) {
+          if (!(ok = take(b & 3, k, 2 + (b >> 2)) && take((b + 1) & 3, k, 2 + (b >> 2)))) break;
 #pragma unroll
-            for (int h = 0; h < 2; h++)
-              tc_mma_ts(d, tmem + kColY + 16u * idx + 8u * h,
-                        tile_desc(kInverse ? 32 + h : 36 + 2 * idx + h), kIdescU8, h);
-          }
-          tc_commit(d_full(b));
-          use[b]++;
+          for (int h = 0; h < 2; h++)
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+              const int bb = b + (r >> 1), g = bb & 3;
+              const int n = 4 * g + 2 * (bb >> 2) + (r & 1);
+              const uint32_t d = tmem + kColD0 + 64u * g + 32u * (r & 1);
+              tc_mma_ts(d, tmem + kColY + 16u * n + 8u * h,
+                        tile_desc(kInverse ? 32 + h : 36 + 2 * n + h), kIdescU8, h);
+            }
+          tc_commit(d_full(b & 3));
+          tc_commit(d_full((b + 1) & 3));
         }
       }
       // every MMA issued above has completed before tensor memory is freed
@@ -320,128 +361,135 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
       ok &= mbar_wait_bounded(drain, 0, kWaitNs);
     }
   } else {
-    // ---- warps 0-7: tensor memory <-> registers <-> shared memory ----
-    const int half = warp >> 2, lq = warp & 3;
+    // ---- warps 0-15: tensor memory <-> registers <-> shared memory ----
+    const int g = warp >> 2, lq = warp & 3;
     const uint32_t lanes = (uint32_t)(32 * lq) << 16;
-    const uint32_t dcol = tmem + lanes + kColD0 + 128u * half;
+    const uint32_t dcol = tmem + lanes + kColD0 + 64u * g;
     const uint32_t ycol = tmem + lanes + kColY;
     const uint32_t p = (uint32_t)(32 * lq + lane);  // polynomial (row) of the tile
     uint32_t use = 0;
     auto take = [&]() {
-      const bool r = mbar_wait_bounded(d_full(half), use & 1u, kWaitNs);
+      const bool r = mbar_wait_bounded(d_full(g), use & 1u, kWaitNs);
       use++;
       tc_fence_after();
-      return r;
+      return __all_sync(0xffffffffu, r);
     };
     auto give_back = [&]() {
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(d_empty(half));
+      if (lane == 0) mbar_arrive(d_empty(g));
+    };
+    // forward: transpose tile t in place into stage 1's operand
+    auto transpose = [&](int t) {
+      const int s = t % kTcSlots;
+      const uint32_t slot = slot_addr(s);
+      const uint32_t mh = (uint32_t)g >> 1, ch = (uint32_t)g & 1u;
+      const bool landed = mbar_wait_bounded(in_full(s), (uint32_t)(t / kTcSlots) & 1u, kWaitNs);
+      uint4 R[8];  // X[8 mh + mm][8 ch .. 8 ch + 7] as four coefficient pairs
+#pragma unroll
+      for (int mm = 0; mm < 8; mm++)
+        R[mm] = ld_shared_v4(sw128_chunk(slot, p, 2u * (8u * mh + mm) + ch));
+      // every warp's rows read before any c-tile is written over them
+      __syncwarp();
+      if (lane == 0) mbar_arrive(x_read);
+      const bool read = mbar_wait_bounded(x_read, (uint32_t)t & 1u, kWaitNs);
+      if (!__all_sync(0xffffffffu, landed && read)) return false;
+#pragma unroll
+      for (int cc = 0; cc < 8; cc++) {
+        const uint32_t sel = (cc & 1) ? 0x7632u : 0x5410u;
+        uint32_t w[4];
+#pragma unroll
+        for (int mp = 0; mp < 4; mp++)
+          w[mp] = __byte_perm(word_of(R[2 * mp], cc >> 1), word_of(R[2 * mp + 1], cc >> 1), sel);
+        st_shared_v4(slot + 4096u * (8u * ch + cc) + (p >> 3) * 256u + (p & 7u) * 16u + 128u * mh,
+                     w[0], w[1], w[2], w[3]);
+      }
+      fence_proxy_async_smem();  // generic-proxy writes -> the tensor cores
+      __syncwarp();
+      if (lane == 0) mbar_arrive(x_ready);
+      return true;
     };
     for (int k = 0; k < nmine && ok; k++) {
-      const int s = k & 1;
+      const int s = k % kTcSlots;
       const uint32_t slot = slot_addr(s);
-      if (!kInverse) {
-        // transpose the loaded tile in place into stage 1's operand
-        const bool landed = mbar_wait_bounded(in_full(s), (uint32_t)(k >> 1) & 1u, kWaitNs);
-        uint4 R[16];  // X[m][8 half .. 8 half + 7] as four coefficient pairs
-#pragma unroll
-        for (int m = 0; m < 16; m++) R[m] = ld_shared_v4(sw128_chunk(slot, p, 2u * m + half));
-        // every warp's rows read before any c-tile is written over them
-        __syncwarp();
-        if (lane == 0) mbar_arrive(x_read);
-        const bool read = mbar_wait_bounded(x_read, (uint32_t)k & 1u, kWaitNs);
-        if (!__all_sync(0xffffffffu, landed && read)) {
-          ok = false;
-          break;
-        }
-#pragma unroll
-        for (int cc = 0; cc < 8; cc++) {
-          const uint32_t sel = (cc & 1) ? 0x7632u : 0x5410u;
-          uint32_t w[8];
-#pragma unroll
-          for (int mp = 0; mp < 8; mp++) {
-            const uint4 a = R[2 * mp], b = R[2 * mp + 1];
-            const uint32_t wa = (cc >> 1) == 0 ? a.x : (cc >> 1) == 1 ? a.y : (cc >> 1) == 2 ? a.z : a.w;
-            const uint32_t wb = (cc >> 1) == 0 ? b.x : (cc >> 1) == 1 ? b.y : (cc >> 1) == 2 ? b.z : b.w;
-            w[mp] = __byte_perm(wa, wb, sel);
-          }
-          const uint32_t xa = slot + 4096u * (8u * half + cc) + (p >> 3) * 256u + (p & 7u) * 16u;
-          st_shared_v4(xa, w[0], w[1], w[2], w[3]);
-          st_shared_v4(xa + 128u, w[4], w[5], w[6], w[7]);
-        }
-        fence_proxy_async_smem();  // generic-proxy writes -> the tensor cores
-        __syncwarp();
-        if (lane == 0) mbar_arrive(x_ready);
+      if (!kInverse && k == 0 && !transpose(0)) {
+        ok = false;
+        break;
       }
       // first stage: S = D_lo + 128 D_hi + 2048 q (non-negative, below 2^25)
-      // as int32 to tensor memory column 16 n + idx (output n of the MMA,
-      // idx = 4j + u its position among the tile's first-stage MMAs), the
-      // second stage's K bytes 4 (idx % 8) .. + 3 of step idx / 8; chunks
-      // j = half, half + 2
+      // as int32 to tensor memory column 16 n + idx (output n of result idx),
+      // the second stage's K bytes 4 (idx % 8) .. + 3 of step idx / 8
 #pragma unroll 1
       for (int jj = 0; jj < 2; jj++) {
-        const int j = half + 2 * jj;
-        if (!__all_sync(0xffffffffu, take())) {
+        const uint32_t a = (uint32_t)g + 4u * jj;
+        if (!take()) {
           ok = false;
           break;
         }
-        uint32_t r0[64], r1[64];
-        tc_ld64(dcol, r0);
-        tc_ld64(dcol + 64, r1);
-        tc_wait_ld();
+        uint32_t r[64];
+        tc_ld64_sync(dcol, r);
         give_back();
 #pragma unroll
         for (int n = 0; n < 16; n++)
-          tc_st4(ycol + 16u * n + 4u * j, r0[n] + (r0[16 + n] << 7) + kFirstBias,
-                 r0[32 + n] + (r0[48 + n] << 7) + kFirstBias,
-                 r1[n] + (r1[16 + n] << 7) + kFirstBias, r1[32 + n] + (r1[48 + n] << 7) + kFirstBias);
+          tc_st2(ycol + 16u * n + 2u * a, r[n] + (r[16 + n] << 7) + kFirstBias,
+                 r[32 + n] + (r[48 + n] << 7) + kFirstBias);
       }
       if (!ok) break;
       tc_wait_st();
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(y_full);
-      // second stage: reduce, pack, write the output rows into the slot
+      if (!kInverse && k + 1 < nmine && !transpose(k + 1)) {
+        ok = false;
+        break;
+      }
+      // second stage: reduce, pack, write the output rows over the tile's
+      // own slot (its first-stage MMAs have completed)
+      if (kInverse) {
+        // results 4g .. 4g + 3 = coefficients 16 i + 4g .. + 3 of every
+        // block i, two per chunk.  Each chunk's pair is stored as soon as it
+        // is reduced: a build that kept the first chunk's packed words in
+        // registers across the wait for the second chunk stored the second
+        // chunk's words in both halves.
 #pragma unroll 1
-      for (int jj = 0; jj < 2; jj++) {
-        const int j = half + 2 * jj;
-        if (!__all_sync(0xffffffffu, take())) {
-          ok = false;
-          break;
-        }
-        if (kInverse) {
-          // coefficients 16 i + c0 .. +3 of every block i (c0 = 8 half + 4 jj):
-          // 8 bytes at byte 8 jj of 16-byte chunk 2 i + half
-          uint32_t r0[64], r1[64];
-          tc_ld64(dcol, r0);
-          tc_ld64(dcol + 64, r1);
-          tc_wait_ld();
-          give_back();
-#pragma unroll
-          for (int i = 0; i < 16; i++) {
-            const uint32_t w0 = pack2(red_centred(r0[i] + (r0[16 + i] << 7)),
-                                      red_centred(r0[32 + i] + (r0[48 + i] << 7)));
-            const uint32_t w1 = pack2(red_centred(r1[i] + (r1[16 + i] << 7)),
-                                      red_centred(r1[32 + i] + (r1[48 + i] << 7)));
-            st_shared_v2(sw128_chunk(slot, p, 2u * i + half) + 8u * jj, w0, w1);
+        for (int jj = 0; jj < 2; jj++) {
+          if (!take()) {
+            ok = false;
+            break;
           }
-        } else {
-          uint32_t r0[64], r1[64];
-          tc_ld64(dcol, r0);
-          tc_ld64(dcol + 64, r1);
-          tc_wait_ld();
+          uint32_t r[64];
+          tc_ld64_sync(dcol, r);
           give_back();
-          // blocks 4j .. 4j+3, each 16 coefficients = two 16-byte chunks
+          // coefficients 16 i + 4g + 2jj, + 1: 4 bytes at byte 8 (g % 2) +
+          // 4 jj of 16-byte chunk 2i + g / 2
+          const uint32_t off = 8u * (g & 1) + 4u * jj;
 #pragma unroll
-          for (int u = 0; u < 4; u++) {
-            const uint32_t* r = u < 2 ? r0 + 32 * u : r1 + 32 * (u - 2);
+          for (int i = 0; i < 16; i++)
+            st_shared_u32(sw128_chunk(slot, p, 2u * i + ((uint32_t)g >> 1)) + off,
+                          pack2(red_centred(r[i] + (r[16 + i] << 7)),
+                                red_centred(r[32 + i] + (r[48 + i] << 7))));
+        }
+      } else {
+        // results = blocks 4g + 2jj, + 1, each 16 coefficients = two 16-byte
+        // chunks
+#pragma unroll 1
+        for (int jj = 0; jj < 2; jj++) {
+          if (!take()) {
+            ok = false;
+            break;
+          }
+          uint32_t r[64];
+          tc_ld64_sync(dcol, r);
+          give_back();
+#pragma unroll
+          for (int u = 0; u < 2; u++) {
+            const uint32_t* ru = r + 32 * u;
             uint32_t w[8];
 #pragma unroll
             for (int t = 0; t < 8; t++)
-              w[t] = pack2(red_exact(r[2 * t] + (r[16 + 2 * t] << 7)),
-                           red_exact(r[2 * t + 1] + (r[17 + 2 * t] << 7)));
-            const uint32_t i = 4u * j + u;
+              w[t] = pack2(red_exact(ru[2 * t] + (ru[16 + 2 * t] << 7)),
+                           red_exact(ru[2 * t + 1] + (ru[17 + 2 * t] << 7)));
+            const uint32_t i = 4u * g + 2u * jj + u;
             st_shared_v4(sw128_chunk(slot, p, 2u * i), w[0], w[1], w[2], w[3]);
             st_shared_v4(sw128_chunk(slot, p, 2u * i + 1), w[4], w[5], w[6], w[7]);
           }

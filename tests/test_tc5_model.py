@@ -197,32 +197,43 @@ def test_stage_a_operand_reads_stay_in_its_quarter():
 
 
 def test_forward_transposition_layout():
-    """In-place transposition of a loaded tile: warp half h reads chunk 2m + h
-    (coefficients 8h .. 8h+7 of block m) of its row from the swizzled slot and
-    writes c-tile c = 8h + cc at 4096 c + (p / 8) 256 + (p % 8) 16 + 128 kc,
-    K bytes 16 kc .. 16 kc + 15 = blocks 8 kc .. 8 kc + 7 of coefficient c.
-    Checked: the reads cover the slot once, the writes cover it once, and a
-    K-major no-swizzle descriptor (LBO 128, SBO 256) at 4096 c reads back
-    X[m][c] for K byte 2m + b of row p."""
+    """In-place transposition of a loaded tile by the four warps of a lane
+    quarter: group g (mh = g / 2, ch = g % 2) reads chunks 2 (8 mh + mm) + ch
+    (coefficients 8 ch .. 8 ch + 7 of blocks 8 mh .. 8 mh + 7) of its row from
+    the swizzled slot and writes c-tile c = 8 ch + cc at 4096 c + (p / 8) 256 +
+    (p % 8) 16 + 128 mh, K bytes 16 mh .. 16 mh + 15 = blocks 8 mh .. 8 mh + 7
+    of coefficient c.  Checked: the reads cover the slot once, the writes cover
+    it once, a K-major no-swizzle descriptor (LBO 128, SBO 256) at 4096 c reads
+    back X[m][c] for K byte 2m + b of row p, and the eight lanes of one
+    shared-memory wavefront (rows p .. p + 7) touch eight distinct 16-byte
+    bank groups on both sides."""
     reads = np.zeros(65536, dtype=np.int64)
     writes = np.zeros(65536, dtype=np.int64)
     for p in range(128):
-        for h in range(2):
-            for m in range(16):
-                k = 2 * m + h
+        for g in range(4):
+            mh, ch = g >> 1, g & 1
+            for mm in range(8):
+                m = 8 * mh + mm
+                k = 2 * m + ch
                 a = (k >> 3) * 16384 + p * 128 + (((k & 7) ^ (p & 7)) << 4)
                 reads[a:a + 16] += 1
+                # the 16 bytes are coefficients 8 ch .. 8 ch + 7 of block m
+                assert (64 * (k >> 3) * 2 + 16 * (k & 7)) // 32 == m
             for cc in range(8):
-                c = 8 * h + cc
-                for kc in range(2):
-                    a = 4096 * c + (p >> 3) * 256 + (p & 7) * 16 + 128 * kc
-                    writes[a:a + 16] += 1
-                    for kb in range(16):        # descriptor view of the same byte
-                        kbyte = 16 * kc + kb
-                        d = 4096 * c + (p // 8) * 256 + (kbyte // 16) * 128 + (p % 8) * 16 + kbyte % 16
-                        assert d == a + kb
-                        assert kbyte // 2 < 16                      # block m = kbyte / 2
+                c = 8 * ch + cc
+                a = 4096 * c + (p >> 3) * 256 + (p & 7) * 16 + 128 * mh
+                writes[a:a + 16] += 1
+                for kb in range(16):        # descriptor view of the same byte
+                    kbyte = 16 * mh + kb
+                    d = 4096 * c + (p // 8) * 256 + (kbyte // 16) * 128 + (p % 8) * 16 + kbyte % 16
+                    assert d == a + kb
+                    assert kbyte // 2 == 8 * mh + kb // 2          # block m = kbyte / 2
     assert (reads == 1).all() and (writes == 1).all()
+    for p0 in range(0, 128, 8):
+        for k in range(32):
+            groups = {((((k & 7) ^ (p & 7)) << 4) % 128) // 16 for p in range(p0, p0 + 8)}
+            assert len(groups) == 8
+        assert len({((p & 7) * 16) // 16 for p in range(p0, p0 + 8)}) == 8
 
 
 def test_forward_output_addresses_are_the_tma_swizzle_layout():
