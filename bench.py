@@ -413,7 +413,11 @@ def run_ours(args):
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_kind == "measured" else "fallback 6650 GB/s",
-                         "bytes_per_launch": BYTES_PER_POLY * n},
+                         "bytes_per_launch": BYTES_PER_POLY * n,
+                         "traffic_how": "ncu --cache-control none on this kernel at 262144 "
+                                        "polynomials (bench.py --traffic): the launch's DRAM "
+                                        "read + write plus the write-back drained after it, "
+                                        "per polynomial, times this launch's polynomials"},
             "kernels_ms": {"ntt_fwd_avg": fwd_avg, "ntt_inv_avg": inv_avg,
                            "ntt_fwd_isolated": fwd_iso, "ntt_inv_isolated": inv_iso,
                            "how": "avg: K2 launches of one kernel back to back between two "
