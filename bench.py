@@ -62,8 +62,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=6.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--variant", type=int, default=-1,
-                   help="force a kernel variant in both directions (-1: auto; 4 is inverse only "
-                        "and then forces only the inverse)")
+                   help="force a kernel variant in both directions (-1: auto; 0-3 mma.sync "
+                        "shapes, 4 tcgen05)")
     p.add_argument("--fwd-variant", type=int, default=-1, help="force the forward's variant")
     p.add_argument("--inv-variant", type=int, default=-1, help="force the inverse's variant")
     p.add_argument("--sweep", action="store_true",
@@ -281,7 +281,7 @@ def run_reference(args):
 def apply_variants(tk, args):
     fwd = args.fwd_variant if args.fwd_variant >= 0 else args.variant
     inv = args.inv_variant if args.inv_variant >= 0 else args.variant
-    if fwd >= 0 and fwd != 4:
+    if fwd >= 0:
         tk.set_variant(tk.FORWARD, fwd)
     if inv >= 0:
         tk.set_variant(tk.INVERSE, inv)
