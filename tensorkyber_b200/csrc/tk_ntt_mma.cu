@@ -480,8 +480,13 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn, kWide>::kMinBlocks)
 
   const int q4 = lane & 3, g8 = lane >> 2;
   // ldmatrix.trans rows of the stage over m: matrix j = lane/8 covers
-  // m = (lane&7) + 8*(j&1), coefficients 8*(j>>1) .. +7.
-  const uint32_t ldt_off = 32u * ((lane & 7) + 8 * ((lane >> 3) & 1)) + 16u * (lane >> 4);
+  // m = (lane&7) + 8*(j&1), coefficients 8*(j>>1) .. +7.  The inverse's
+  // intermediate (stage A's output) keeps the two 16-byte coefficient halves
+  // of block m swapped when bit 2 of m is set, so that the eight rows of each
+  // matrix (m = 0..7 or 8..15, 32 bytes apart) fall on eight different bank
+  // groups instead of two rows per group.
+  const uint32_t ldt_off = 32u * ((lane & 7) + 8 * ((lane >> 3) & 1)) +
+                           16u * ((lane >> 4) ^ (kInverse ? (lane >> 2) & 1 : 0));
   // forward stage-1 stores: block i = lane/4 (and +8); the parity halves are
   // swapped in blocks with bit 2 set (bank spread).
   const uint32_t hb1 = (lane >> 4) & 1;
@@ -494,7 +499,10 @@ __global__ void __launch_bounds__(32 * W, Cfg<W, S, kIn, kWide>::kMinBlocks)
   const uint32_t hbw = (uint32_t)((blk0 >> 2) & 1);
   const uint32_t ldc_off = kRowBytes * (lane & 7) + 32u * (lane >> 4) +
                            16u * (kInverse ? ((lane >> 3) & 1) : (((lane >> 3) & 1) ^ hbw));
-  const uint32_t stc_off = kRowBytes * (2 * q4) + 4u * g8;  // output pair lane/4, polys 2q, 2q+1
+  // block-wise stage output: coefficient pair lane/4 of polynomials 2q, 2q+1;
+  // the inverse's (the intermediate) with the halves swapped in blocks with
+  // bit 2 set (the warp's blocks share that bit: hbw)
+  const uint32_t stc_off = kRowBytes * (2 * q4) + 4u * (g8 ^ (kInverse ? 4 * hbw : 0));
   // wide kernels: stage-1 stores of block lane/4 (even / odd half, swizzled),
   // and the stage-2 ldmatrix rows of each block pair
   const uint32_t swz1 = (uint32_t)(g8 >> 1) & 1u;
@@ -805,6 +813,11 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
   const uint32_t ldc_fwd = ldc_base + 16u * (((lane >> 3) & 1) ^ hbw);
   const uint32_t ldc_inv = ldc_base + 16u * ((lane >> 3) & 1);
   const uint32_t stc_off = kRowBytes * (2 * q4) + 4u * g8;
+  // the inverse's intermediate with block halves swapped where bit 2 of the
+  // block is set (as the batch kernel's): stage A's stores, stage B's rows
+  const uint32_t stc_inv = kRowBytes * (2 * q4) + 4u * (g8 ^ (4 * hbw));
+  const uint32_t ldt_inv = 32u * ((lane & 7) + 8 * ((lane >> 3) & 1)) +
+                           16u * ((lane >> 4) ^ ((lane >> 2) & 1));
 
   auto batch_of = [&](int t) {
     int b = 0;
@@ -888,7 +901,7 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
     {
       uint32_t iac[PP][2][2][2];
       load_ac(g_inv.sa, iac);
-      block_stage<true, W, PP, NU>(acc, accp, blk0, ldc_inv, stc_off, iac, zc);
+      block_stage<true, W, PP, NU>(acc, accp, blk0, ldc_inv, stc_inv, iac, zc);
     }
     cta_sync_named();
     if (warp < NU) {
@@ -903,7 +916,7 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
         cb[t][2] = (int32_t)v.z;
         cb[t][3] = (int32_t)v.w;
       }
-      poly_stage<true, true>(acc + 8 * warp * kRowBytes, accp + 8 * warp * kRowBytes, ldt_off, iam,
+      poly_stage<true, true>(acc + 8 * warp * kRowBytes, accp + 8 * warp * kRowBytes, ldt_inv, iam,
                              0, 0, cb, 0, 0, w_nat, P.e[b], row0 + 8 * warp, nvec, 8u * g8 + q4);
       fence_proxy_async_smem();
       __syncwarp();
