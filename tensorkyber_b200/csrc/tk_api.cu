@@ -83,7 +83,11 @@ int choose_variant(bool inverse, size_t npoly) {
   if (f >= 0) return f;
   const int t = g_tuned[inverse ? 1 : 0][size_bucket(npoly)].load(std::memory_order_relaxed);
   if (t >= 0) return t;
-  return inverse ? (npoly >= ((size_t)1 << 19) ? 2 : 0) : 3;
+  // untuned: the measured best per direction (forward: the int32-tile
+  // mma.sync kernel everywhere; inverse: the tcgen05 kernel from 2^18
+  // polynomials, where it leads, the 3-slot mma.sync kernel below, where the
+  // tcgen05 kernel's larger CTA costs more to start)
+  return inverse ? (npoly >= ((size_t)1 << 18) ? tk::kTc5Variant : 0) : 3;
 }
 
 void set_err(const char* what, cudaError_t e) {

@@ -34,22 +34,25 @@
 //     written in the TMA layout over the tile's own input slot (its MMAs have
 //     finished), and TMA stores the tile.
 //
-// Roles (576 threads, one CTA per SM by shared memory): warp 17 lane 0
-// issues TMA loads and stores; warp 16 lane 0 issues MMAs (and warp 16 owns
-// the tensor-memory allocation); warps 0-15 move data between tensor memory,
-// registers and shared memory in four groups of four, warp w reaching
-// tensor-memory lanes 32 (w % 4) .. + 31 (polynomials).  Tensor memory (512
-// columns): 0-255 the first stage's sums, 256 + 64 g .. + 63 group g's
-// accumulator buffer (two 32-column MMA results).  Per tile the MMA thread
-// issues 16 chunks of two results, chunk j into buffer j % 4, so the MMAs of
-// one group's chunk run while the other groups read theirs, and the next
-// tile's first stage starts while this tile's second-stage results are still
-// being read.  Three slots of 64 KiB: the load of tile k + 3 goes into tile
-// k's slot once tile k's output (written over its input) has been read out
-// by the store.  Every mbarrier wait gives up after 2 s (status bit 0
-// forward / 1 inverse, as the other kernels); the MMA thread then drains its
-// MMAs and the producer its copies before the CTA frees tensor memory and
-// exits.
+// Roles (608 threads, one CTA per SM by shared memory): warp 18 lane 0
+// issues TMA loads and stores; lane 0 of warps 16 and 17 issue MMAs, warp
+// 16 + j for the chunks of groups j and j + 2 (one issuing thread could not
+// keep the tensor pipe fed: it shares its SMSP with busy epilogue warps), and
+// warp 16 owns the tensor-memory allocation; warps 0-15 move data between
+// tensor memory, registers and shared memory in four groups of four, warp w
+// reaching tensor-memory lanes 32 (w % 4) .. + 31 (polynomials).  Tensor
+// memory (512 columns): 0-255 the first stage's sums, 256 + 64 g .. + 63
+// group g's accumulator buffer (two 32-column MMA results).  Per tile 16
+// chunks of two results go out, chunk j into buffer j % 4, so the MMAs of one
+// group's chunk run while the other groups read theirs, and the next tile's
+// first stage starts while this tile's second-stage results are still being
+// read (an mbarrier, y_free, keeps the next tile's sums from being written
+// before both issuers' second-stage MMAs of this tile have read them).
+// Three slots of 64 KiB: the load of tile k + 3 goes into tile k's slot once
+// tile k's output (written over its input) has been read out by the store.
+// Every mbarrier wait gives up after 2 s (status bit 0 forward / 1 inverse,
+// as the other kernels); the issuers then drain their MMAs and the producer
+// its copies before the CTA frees tensor memory and exits.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
@@ -72,14 +75,20 @@ constexpr int kTcSlots = 3;
 // lane quarter) owns accumulator buffer g
 constexpr int kTcGroups = 4;
 constexpr int kTcEpiWarps = 4 * kTcGroups;
-constexpr int kTcMmaWarp = kTcEpiWarps, kTcTmaWarp = kTcEpiWarps + 1;
-constexpr int kTcThreads = 32 * (kTcEpiWarps + 2);
+// MMA issuers: warp kTcMmaWarp + j issues the chunks of groups j and j + 2
+// (two SMSPs, so that no single thread has to keep the tensor pipe fed
+// against the epilogue warps' instructions); the first also owns the TMEM
+// allocation.  19 warps: registers are allocated for 20, 96 per thread.
+constexpr int kTcIssuers = 2;
+constexpr int kTcMmaWarp = kTcEpiWarps, kTcTmaWarp = kTcEpiWarps + kTcIssuers;
+constexpr int kTcThreads = 32 * (kTcEpiWarps + kTcIssuers + 1);
 // dynamic shared memory (its base is 1024-byte aligned, the swizzle atom;
 // the kernel checks): three 64 KiB tile slots, this direction's constant
 // tiles, the mbarriers (in_full[3], out_ready[3], d_full[4], d_empty[4],
-// y_full, x_ready, x_read, consts, drain) and the tensor-memory base address
+// y_full, x_ready, x_read, consts, drain, y_free) and the tensor-memory base
+// address
 constexpr int kOffTables = kTcSlots * kTcSlotBytes;
-constexpr int kNumBars = 2 * kTcSlots + 2 * kTcGroups + 5;
+constexpr int kNumBars = 2 * kTcSlots + 2 * kTcGroups + 6;
 template <bool kInverse>
 struct Tc5Layout {
   static constexpr int kTiles = kInverse ? kTc5InvTiles : kTc5FwdTiles;
@@ -197,7 +206,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
   auto d_empty = [&](int g) { return bars + 8u * (2 * kTcSlots + kTcGroups + g); };
   constexpr uint32_t kB = 8u * (2 * kTcSlots + 2 * kTcGroups);
   const uint32_t y_full = bars + kB, x_ready = bars + kB + 8u, x_read = bars + kB + 16u,
-                 consts = bars + kB + 24u, drain = bars + kB + 32u;
+                 consts = bars + kB + 24u, drain = bars + kB + 32u, y_free = bars + kB + 40u;
   auto slot_addr = [&](int s) { return base + (uint32_t)s * kTcSlotBytes; };
 
   if (tid == 0) {
@@ -213,10 +222,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
     mbar_init(x_ready, kTcEpiWarps);
     mbar_init(x_read, kTcEpiWarps);
     mbar_init(consts, 1);
-    mbar_init(drain, 1);
+    mbar_init(drain, kTcIssuers);
+    mbar_init(y_free, kTcIssuers);
     fence_mbar_init();
   }
-  if (warp == kTcMmaWarp) {
+  if (warp == kTcMmaWarp) {  // the first issuer's warp
     tmem_alloc(base + L::kOffTmemSlot, kTmemCols);
     tmem_relinquish();
   }
@@ -267,25 +277,23 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
           ok &= mbar_wait_bounded(in_full(s), (uint32_t)(last_load[s] / kTcSlots) & 1u, kWaitNs);
       ok &= mbar_wait_bounded(consts, 0, kWaitNs);
     }
-  } else if (warp == kTcMmaWarp) {
+  } else if (warp >= kTcMmaWarp) {
     if (lane == 0) {
-      // ---- MMA issuer ----
-      // One thread issues every MMA, so its instruction chain per MMA sets
-      // the issue rate: descriptors are built once (a shared-memory
-      // descriptor's low 14 bits are the address / 16, so an operand at
-      // byte offset o is the base descriptor + o / 16; every address here is
-      // below 2^18) and the chunk loops are unrolled, leaving an add and the
-      // MMA per operand pair.
+      // ---- MMA issuer j: the chunks of groups j and j + 2 ----
+      // Descriptors are built once (a shared-memory descriptor's low 14 bits
+      // are the address / 16, so an operand at byte offset o is the base
+      // descriptor + o / 16; every address here is below 2^18).
+      const int j = warp - kTcMmaWarp;
       const uint64_t b_desc0 = smem_desc(tables, 128, 256, kLayoutNone);
       auto tile_desc = [&](int i) {
         return b_desc0 + (uint64_t)((i - L::kFirstTile) * (kTc5TileBytes >> 4));
       };
       const uint64_t a_desc0 = kInverse ? smem_desc(base, 16, 1024, kLayoutSw128)
                                         : smem_desc(base, 128, 256, kLayoutNone);
-      // buffer g's previous contents were read out: every tile uses each
-      // buffer four times (first-stage chunks g, g + 4, second-stage chunks
-      // g, g + 4), so the use at position pos (0..3) of tile k is use 4k +
-      // pos and waits for the release of use 4k + pos - 1
+      // buffer g's previous contents were read out: every tile uses it four
+      // times (first-stage chunks g, g + 4, second-stage chunks g, g + 4), so
+      // the use at position pos (0..3) of tile k is use 4k + pos and waits
+      // for the release of use 4k + pos - 1
       auto take = [&](int g, int k, int pos) {
         if ((k > 0 || pos > 0) && !mbar_wait_bounded(d_empty(g), (uint32_t)(pos + 1) & 1u, kWaitNs))
           return false;
@@ -304,57 +312,55 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
         if (!ok) break;
         tc_fence_after();
         const uint64_t a_slot = a_desc0 + (uint64_t)(s * (kTcSlotBytes >> 4));
-        // first stage: chunk a = results 2a, 2a + 1 (inverse: blocks of input
-        // quarter a / 2; forward: c-tiles), an MMA pair each.  Chunks go out
-        // two at a time, the first MMA of all four results before any second
-        // one: the second accumulates onto the first's result and waits for
-        // it, and the tensor pipe issues in order, so the four independent
-        // first MMAs cover that latency.
+        // first stage: chunk a = g + 4 jj (g = j, j + 2) = results 2a, 2a + 1
+        // (inverse: blocks; forward: c-tiles), an MMA pair each, both
+        // results' first MMA before either second one; chunks in order a =
+        // j, j + 2, j + 4, j + 6
 #pragma unroll
-        for (int a = 0; a < 8; a += 2) {
-          if (!(ok = take(a & 3, k, a >> 2) && take((a + 1) & 3, k, a >> 2))) break;
+        for (int c = 0; c < 4; c++) {
+          const int g = j + 2 * (c & 1), jj = c >> 1, a = g + 4 * jj;
+          if (!(ok = take(g, k, jj))) break;
+          const uint32_t dbuf = tmem + kColD0 + 64u * (uint32_t)g;
 #pragma unroll
-          for (int t = 0; t < 2; t++) {
+          for (int t = 0; t < 2; t++)
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-              const int idx = 2 * a + r, g = (a + (r >> 1)) & 3;
-              const uint32_t d = tmem + kColD0 + 64u * g + 32u * (r & 1);
-              if (kInverse) {
-                const uint64_t ad =
-                    a_slot + (uint64_t)(((idx >> 2) * kTcQuarterBytes + 32 * (idx & 3)) >> 4);
-                tc_mma_ss(d, ad, tile_desc(2 * idx + t), t ? kIdescS8 : kIdescU8, t);
-              } else {
-                const uint64_t ad = a_slot + (uint64_t)((4096 * idx) >> 4);
-                tc_mma_ss(d, ad, tile_desc(34 + t), t ? kIdescS8 : kIdescU8, t);
-              }
+            for (int u = 0; u < 2; u++) {
+              const int idx = 2 * a + u;
+              const uint64_t ad =
+                  kInverse
+                      ? a_slot + (uint64_t)(((idx >> 2) * kTcQuarterBytes + 32 * (idx & 3)) >> 4)
+                      : a_slot + (uint64_t)((4096 * idx) >> 4);
+              tc_mma_ss(dbuf + 32u * u, ad, tile_desc(kInverse ? 2 * idx + t : 34 + t),
+                        t ? kIdescS8 : kIdescU8, t);
             }
-            if (t == 1) {
-              tc_commit(d_full(a & 3));
-              tc_commit(d_full((a + 1) & 3));
-            }
-          }
+          tc_commit(d_full(g));
         }
         if (!ok) break;
-        // second stage from tensor memory, two K steps per result, in the
-        // same order (chunks b, b + 1: both results' K step 0, then step 1)
+        // second stage from tensor memory, two K steps per result: chunk b =
+        // g + 4 jj = results n = 4g + 2 jj, + 1
         if (!(ok = mbar_wait_bounded(y_full, (uint32_t)k & 1u, kWaitNs))) break;
         tc_fence_after();
 #pragma unroll
-        for (int b = 0; b < 8; b += 2) {
-          if (!(ok = take(b & 3, k, 2 + (b >> 2)) && take((b + 1) & 3, k, 2 + (b >> 2)))) break;
+        for (int c = 0; c < 4; c++) {
+          const int g = j + 2 * (c & 1), jj = c >> 1;
+          if (!(ok = take(g, k, 2 + jj))) break;
+          const uint32_t dbuf = tmem + kColD0 + 64u * (uint32_t)g;
+          const int n0 = 4 * g + 2 * jj;
 #pragma unroll
           for (int h = 0; h < 2; h++)
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-              const int bb = b + (r >> 1), g = bb & 3;
-              const int n = 4 * g + 2 * (bb >> 2) + (r & 1);
-              const uint32_t d = tmem + kColD0 + 64u * g + 32u * (r & 1);
-              tc_mma_ts(d, tmem + kColY + 16u * n + 8u * h,
+            for (int u = 0; u < 2; u++) {
+              const int n = n0 + u;
+              tc_mma_ts(dbuf + 32u * u, tmem + kColY + 16u * (uint32_t)n + 8u * h,
                         tile_desc(kInverse ? 32 + h : 36 + 2 * n + h), kIdescU8, h);
             }
-          tc_commit(d_full(b & 3));
-          tc_commit(d_full((b + 1) & 3));
+          tc_commit(d_full(g));
         }
+        if (!ok) break;
+        // this issuer's reads of the first stage's sums are issued: the
+        // barrier completes when both issuers' have finished, after which the
+        // next tile's sums may be written over them
+        tc_commit(y_free);
       }
       // every MMA issued above has completed before tensor memory is freed
       tc_commit(drain);
@@ -418,14 +424,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
       }
       // first stage: S = D_lo + 128 D_hi + 2048 q (non-negative, below 2^25)
       // as int32 to tensor memory column 16 n + idx (output n of result idx),
-      // the second stage's K bytes 4 (idx % 8) .. + 3 of step idx / 8
+      // the second stage's K bytes 4 (idx % 8) .. + 3 of step idx / 8.  The
+      // previous tile's second-stage MMAs (from every issuer) read these
+      // columns: y_free says they have finished.
 #pragma unroll 1
       for (int jj = 0; jj < 2; jj++) {
         const uint32_t a = (uint32_t)g + 4u * jj;
-        if (!take()) {
+        if (!take() ||
+            (jj == 0 && k > 0 &&
+             !__all_sync(0xffffffffu, mbar_wait_bounded(y_free, (uint32_t)(k - 1) & 1u, kWaitNs)))) {
           ok = false;
           break;
         }
+        if (jj == 0 && k > 0) tc_fence_after();
         uint32_t r[64];
         tc_ld64_sync(dcol, r);
         give_back();
@@ -504,7 +515,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
   tc_fence_before();
   __syncthreads();
   if (warp == kTcMmaWarp) {
-    __syncwarp();  // lane 0 issued the MMAs alone; dealloc is warp-wide
+    __syncwarp();  // lane 0 issued MMAs alone; dealloc is warp-wide
     tc_fence_after();
     tmem_dealloc(tmem, kTmemCols);
   }
