@@ -89,6 +89,17 @@ def test_variant_selection(tk):
     assert "tcgen05" in tk.variant_name(4)
 
 
+def test_untuned_defaults(tk):
+    """Without forcing or tuning: the int32-tile mma.sync forward (3) at every
+    size; the inverse on the 3-slot mma.sync kernel (0) below 2^18
+    polynomials and on the tcgen05 kernel (4) from there, where it leads."""
+    for d in (tk.FORWARD, tk.INVERSE):
+        tk.set_variant(d, -1)
+    for n in (1, 4096, (1 << 18) - 1, 1 << 18, 1 << 24):
+        assert tk.get_variant(tk.FORWARD, n) == 3
+        assert tk.get_variant(tk.INVERSE, n) == (4 if n >= (1 << 18) else 0)
+
+
 def test_get_table_sizes(tk):
     L = tk.lib()
     assert L.tk_get_table(0, None, 0) == 16 * 16 * 2
