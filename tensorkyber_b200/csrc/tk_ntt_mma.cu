@@ -944,7 +944,7 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
     const int t = (int)blockIdx.x + k * G, b = batch_of(t), tl = t - P.first_tile[b];
     const int kb = P.k[b];  // CTA-uniform
     const int row0 = tl * 8 * tile_units(kb), nvec = P.njobs[b] * kb;
-    if (kb == 3)
+    if (tile_units(kb) == 3)  // the phase code for the tile's unit count
       fwd_phase(U3{}, slot, slotp);
     else
       fwd_phase(U4{}, slot, slotp);
@@ -956,7 +956,7 @@ __global__ void __launch_bounds__(128, 4) k_matvec_tiles(const __grid_constant__
       default: basemul_phase(std::integral_constant<int, 4>{}, b, tl, slotp); break;
     }
     cta_sync_named();
-    if (kb == 3)
+    if (tile_units(kb) == 3)  // the phase code for the tile's unit count
       inv_phase(U3{}, b, row0, nvec);
     else
       inv_phase(U4{}, b, row0, nvec);
