@@ -163,12 +163,13 @@ __device__ __forceinline__ uint32_t sw128_chunk(uint32_t slot, uint32_t p, uint3
   return slot + (k >> 3) * kTcQuarterBytes + p * 128u + (((k & 7u) ^ (p & 7u)) << 4);
 }
 
-// Per tile the MMA thread issues 16 chunks of two 32-column MMA results:
+// Per tile the two issuers send 16 chunks of two 32-column MMA results:
 // first stage a = 0..7 (results 2a, 2a + 1: inverse blocks, forward
 // coefficients), second stage b = 0..7 (results n = 4 (b % 4) + 2 (b / 4) and
 // n + 1: inverse coefficients, forward blocks); chunk a or b goes to buffer
-// (and warp group) a % 4 or b % 4, so group g reads first-stage chunks g, g+4
-// and the second-stage results 4g .. 4g + 3.  The MMAs of one chunk can run
+// (and warp group) a % 4 or b % 4, issued by issuer (a or b) % 2, so group g
+// reads first-stage chunks g, g+4 and the second-stage results 4g .. 4g + 3.
+// The MMAs of one chunk can run
 // while the other groups read theirs; the second stage waits for the whole
 // first stage in tensor memory (y_full), the next tile's first stage only
 // for its buffers.
