@@ -14,7 +14,7 @@
 //     x 128 rows with the 128-byte swizzle, which is exactly the canonical
 //     K-major SW128 operand layout: the inverse's stage-A A operand for block
 //     m is the 32 bytes of that block in each row, read straight from the
-//     loaded tile.  The forward contracts over m first, so the 8 epilogue
+//     loaded tile.  The forward contracts over m first, so the 16 epilogue
 //     warps transpose the tile in place into stage 1's operand (K-major
 //     without swizzle) before its MMAs.
 //   * Signed data need no CUDA-core pass.  An int16 x = b0 + 256 b1 with b0
