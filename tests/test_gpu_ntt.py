@@ -448,3 +448,25 @@ def test_headline_size_every_forward_variant(tk, cuda, oracle, variant):
         tk.set_variant(tk.FORWARD, -1)
     check_fwd(out, oracle.ntt(canon(x).astype(np.int16)))
     assert tk.device_status(0) == 0
+
+
+@pytest.mark.parametrize("n", [(1 << 18) - 1, (1 << 18) + 1])
+def test_default_inverse_across_the_kernel_switch(tk, cuda, oracle, n):
+    """The untuned inverse runs the mma.sync kernel below 2^18 polynomials and
+    the tcgen05 kernel from there: both sides of the switch, full-range
+    inputs, every coefficient of a spread sample against the oracle and the
+    two kernels byte-equal on the whole batch."""
+    for d in (tk.FORWARD, tk.INVERSE):
+        tk.set_variant(d, -1)
+    assert tk.get_variant(tk.INVERSE, n) == (0 if n < (1 << 18) else TC5)
+    x = rng(7000 + n % 7).integers(-32768, 32768, size=(n, 256), dtype=np.int16)
+    out = gpu_inv(tk, cuda, x)
+    pick = np.unique(np.r_[0:300, n // 2 - 150:n // 2 + 150, n - 300:n])
+    check_inv(out[pick], oracle.invntt(canon(x[pick]).astype(np.int16)))
+    try:
+        tk.set_variant(tk.INVERSE, TC5 if n < (1 << 18) else 0)
+        other = gpu_inv(tk, cuda, x)
+    finally:
+        tk.set_variant(tk.INVERSE, -1)
+    assert (other == out).all()
+    assert tk.device_status(0) == 0
