@@ -470,3 +470,35 @@ def test_default_inverse_across_the_kernel_switch(tk, cuda, oracle, n):
         tk.set_variant(tk.INVERSE, -1)
     assert (other == out).all()
     assert tk.device_status(0) == 0
+
+
+def test_tcgen05_random_sizes_stress(tk, cuda):
+    """120 launches of the tcgen05 kernels at random sizes (log-uniform, 1 ..
+    2^19) and directions, in place and out of place, each byte-equal to the
+    mma.sync kernels on the same input: many tile counts per CTA and ragged
+    last tiles, under whatever timing the GPU gives each launch."""
+    torch = cuda
+    r = np.random.default_rng(31337)
+    try:
+        for it in range(120):
+            n = int(np.exp(r.uniform(0, np.log(1 << 19))))
+            inverse = bool(r.integers(2))
+            d = tk.INVERSE if inverse else tk.FORWARD
+            fn = tk.invntt if inverse else tk.ntt
+            x = torch.from_numpy(r.integers(-32768, 32768, size=(n, 256), dtype=np.int16)).cuda()
+            tk.set_variant(d, 0 if inverse else 3)
+            ref = x.clone()
+            fn(ref)
+            tk.set_variant(d, TC5)
+            if it % 2:
+                got = torch.empty_like(x)
+                fn(x, out=got)
+            else:
+                got = x.clone()
+                fn(got)
+            torch.cuda.synchronize()
+            assert torch.equal(got, ref), (it, n, inverse)
+    finally:
+        for d in (tk.FORWARD, tk.INVERSE):
+            tk.set_variant(d, -1)
+    assert tk.device_status(0) == 0
