@@ -170,7 +170,10 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 }
 
 // ---- modular epilogue helpers ------------------------------------------------
-// S in [0, 2^25): representative in [0, q + 8).
+// S in [0, 2^25): representative in [0, q + 11) (the quotient is floor(S /
+// q) or one less; when it is one less, S mod q is below S (2^32 - q floor(2^32
+// / q)) / 2^32 <= 10.6), [0, q + 6) for S < 2^24.  Either way the high byte of
+// the result is at most 13.
 __device__ __forceinline__ uint32_t red_lazy(uint32_t s) {
   return s - __umulhi(s, 1290167u) * 3329u;
 }

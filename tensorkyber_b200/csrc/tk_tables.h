@@ -39,8 +39,8 @@ namespace tk {
 constexpr int kN = 256;
 constexpr int kQ = 3329;
 
-// floor(2^32 / q): lazy Barrett, S - umulhi(S, kBarLazy) * q in [0, q + 8) for
-// S < 2^25.
+// floor(2^32 / q): lazy Barrett, S - umulhi(S, kBarLazy) * q in [0, q + 11)
+// for S < 2^25, [0, q + 6) for S < 2^24.
 constexpr uint32_t kBarLazy = 1290167u;
 // ceil(2^38 / q): exact reduction floor(S / q) = umulhi(S, kBarExact) >> 6 for
 // every 0 <= S < 2^26 (the error term S * e / 2^38 < 2^-12 < 1/q).

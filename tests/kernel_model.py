@@ -95,7 +95,7 @@ class FwdModel:
             mid = S
         else:
             mid = S - ((S * BAR_LAZY) >> 32) * Q                             # [p][i][c]
-            assert mid.min() >= 0 and mid.max() < Q + 8
+            assert mid.min() >= 0 and mid.max() < Q + 11       # red_lazy below 2^25
         out = np.zeros((P, 256), dtype=np.int64)
         for b in range(16):
             for s in range(2):

@@ -90,3 +90,22 @@ def test_single_limb_stage1_model(tk, oracle, lo, hi, wide):
     x = rng(7 + hi).integers(lo, hi, size=(200, 256)).astype(np.int16)
     x[0], x[1] = lo, hi - 1
     assert (fw(x, single_limb=True, wide=wide) == canon(oracle.ntt(x))).all()
+
+
+def test_lazy_reduction_bound():
+    """red_lazy (S - umulhi(S, floor(2^32 / q)) q) on its whole documented
+    domain, checked on its extremes and a random sample: congruent to S, in
+    [0, q + 11) for S < 2^25 (the top of the range reaches q + 10) and in
+    [0, q + 6) for S < 2^24; the high byte is at most 13 either way."""
+    M = (1 << 32) // Q
+    r = rng(7)
+    for top, bound in ((1 << 25, Q + 11), (1 << 24, Q + 6)):
+        s = np.concatenate([np.arange(0, 1 << 18), np.arange(top - (1 << 20), top),
+                            r.integers(0, top, size=1 << 20)]).astype(np.int64)
+        v = s - ((s * M) >> 32) * Q
+        assert v.min() >= 0 and v.max() < bound and ((v - s) % Q == 0).all()
+        assert v.max() >> 8 <= 13
+    # the error term: when the quotient is one short, S mod q < S e / 2^32
+    # with e = 2^32 - q M
+    e = (1 << 32) - Q * M
+    assert (1 << 25) * e < 11 * (1 << 32) and (1 << 24) * e < 6 * (1 << 32)
