@@ -1223,7 +1223,7 @@ cudaError_t launch_mma_segs(bool inverse, int variant, const Seg* segs, int nseg
     variant = 0;
   }
   // pieces of at most kMaxLaunchPolys, in order
-  Piece pc[kMaxSegs];
+  Piece pc[kMaxSegs] = {};
   int np = 0;
   auto launch_pieces = [&]() -> cudaError_t {
     if (np == 0) return cudaSuccess;
