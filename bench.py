@@ -85,6 +85,8 @@ def parse():
                    help="offered load as multiples of the plain per-request capacity")
     p.add_argument("--serve-templates", type=int, default=256)
     p.add_argument("--serve-zero-copy", action="store_true")
+    p.add_argument("--serve-no-arena", action="store_true",
+                   help="skip the server arm whose requests lie back to back in one pinned arena")
     p.add_argument("--serve-plain-mode", type=int, default=2,
                    help="matrix-vector mode of the plain per-request path (0, 1, 2 as --matvec-mode)")
     p.add_argument("--traffic", action="store_true",
@@ -759,7 +761,7 @@ def run_serve(args):
         o_plain, o_srv = pinned((n, k, 256)), pinned((n, k, 256))
         batch = (tk.MatvecBatch * 1)(tk.MatvecBatch(k, n, A.ctypes.data, sv.ctypes.data,
                                                     e.ctypes.data, o_plain.ctypes.data))
-        tmpl.append(dict(k=k, n=n, A=A, s=sv, e=e, o_plain=o_plain, o_srv=o_srv, batch=batch,
+        tmpl.append(dict(k=k, n=n, A=A, s=sv, e=e, blk=blk, o_plain=o_plain, o_srv=o_srv, batch=batch,
                          ptrs=(A.ctypes.data, sv.ctypes.data, e.ctypes.data, o_srv.ctypes.data)))
     polys = np.array([t["n"] * t["k"] for t in tmpl])
     pc = time.perf_counter
@@ -813,6 +815,30 @@ def run_serve(args):
     arms = {"server": dict(zero_copy=False)}
     if args.serve_zero_copy:
         arms["server_zero_copy"] = dict(zero_copy=True)
+    # server_arena: each rate's requests copied, in arrival order, back to back
+    # into one pinned arena (as a receive ring would hold them), so that the
+    # server's admission passes can take several requests' inputs in one copy
+    msg_bytes = np.array([t["blk"].nbytes for t in tmpl], dtype=np.int64)
+    arena = None
+    if not args.serve_no_arena:
+        need = max(int(msg_bytes[w].sum()) for _, _, w, _ in runs)
+        arena = torch.empty(need // 2, dtype=torch.int16, pin_memory=True).numpy()
+        arms["server_arena"] = dict(zero_copy=False)
+
+    def request_ptrs(name, which):
+        """Per request (A, s, e, out) addresses: the template's own buffers,
+        or for the arena arm its message's place in the filled arena."""
+        if name != "server_arena":
+            return [tmpl[w]["ptrs"] for w in which]
+        offs = np.concatenate([[0], np.cumsum(msg_bytes[which])[:-1]])
+        out, base0 = [], arena.ctypes.data
+        for o, w in zip(offs, which):
+            t = tmpl[w]
+            arena[o // 2:o // 2 + t["blk"].size] = t["blk"].ravel()
+            a = base0 + int(o)
+            sp = a + t["n"] * t["k"] * t["k"] * 512
+            out.append((a, sp, sp + t["n"] * t["k"] * 512, t["ptrs"][3]))
+        return out
     ticket = ctypes.c_uint64()
     stats = {}
     for name, kw in arms.items():
@@ -831,12 +857,13 @@ def run_serve(args):
             nreq = len(arr)
             lag = np.empty(nreq)
             tickets = np.empty(nreq, dtype=np.uint64)
+            ptrs = request_ptrs(name, which)
             base = pc() + 1e-3
             for i in range(nreq):
                 ta = base + arr[i]
                 spin_until(ta)
                 t = tmpl[which[i]]
-                a, b_, c, d = t["ptrs"]
+                a, b_, c, d = ptrs[i]
                 rc = L.tk_server_submit(srv._h, t["k"], t["n"], a, b_, c, d,
                                         ctypes.byref(ticket))
                 lag[i] = pc() - ta
@@ -853,11 +880,14 @@ def run_serve(args):
             split = {f"mean_{x}_us": (st[f"{x}_ns"] - st0[f"{x}_ns"]) / 1e3 /
                      max(1, st["requests_done"] - st0["requests_done"])
                      for x in ("queue", "device", "return")}
+            copies = (st["input_copies"] - st0["input_copies"]) / max(
+                1, st["requests_done"] - st0["requests_done"])
             st0 = st
             pt[name] = {"p50_us": pct(slat, 50), "p99_us": pct(slat, 99),
                         "polys_per_s": tot_polys / (end - base),
                         "requests_per_s": nreq / (end - base),
-                        "submit_lag_p99_us": pct(lag, 99), **split}
+                        "submit_lag_p99_us": pct(lag, 99),
+                        "input_copies_per_request": copies, **split}
         stats[name] = srv.stats()
         srv.close()
     clocks = sampler.stop()
@@ -875,7 +905,10 @@ def run_serve(args):
                                "coefficients uniform [0,q), pinned host buffers (A|s|e contiguous)",
                    "templates": T,
                    "plain_mode": ["pipeline", "fused", "tiled"][args.serve_plain_mode],
-                   "server": "fused warp-per-job device loop"},
+                   "server": "fused warp-per-job device loop",
+                   "arms": {"server": "each request's A|s|e in its own pinned buffer",
+                            "server_arena": "the same requests back to back in one pinned "
+                                            "arena, in arrival order"}},
         "dtype": "int16", "data": "synthetic",
     }), flush=True)
 

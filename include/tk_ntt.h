@@ -177,6 +177,10 @@ typedef struct tk_server_counters {
   unsigned long long direct_requests, staged_requests;  /* inputs in place / staged */
   unsigned long long direct_outputs;                    /* outputs written in place */
   unsigned long long queue_ns, device_ns, return_ns;
+  /* host-to-device copy operations issued for staged inputs: below
+   * staged_requests when the inputs of requests admitted together lie back to
+   * back in one page-locked allocation (they go in one copy) */
+  unsigned long long input_copies;
 } tk_server_counters;
 int tk_server_create(int device, const tk_server_config *cfg, tk_server **out);
 int tk_server_submit(tk_server *srv, int k, size_t njobs, const int16_t *A, const int16_t *s,

@@ -47,7 +47,8 @@ class ServerCounters(ctypes.Structure):
     """Mirror of tk_server_counters (include/tk_ntt.h)."""
     _fields_ = [(n, ctypes.c_ulonglong) for n in (
         "requests_done", "jobs_done", "device_loop_launches", "direct_requests",
-        "staged_requests", "direct_outputs", "queue_ns", "device_ns", "return_ns")]
+        "staged_requests", "direct_outputs", "queue_ns", "device_ns", "return_ns",
+        "input_copies")]
 
 
 class TKError(RuntimeError):

@@ -81,6 +81,10 @@ struct Request {
   bool in_direct = false;   // inputs read in place (zero_copy)
   bool out_direct = false;  // outputs written in place (out is mapped pinned memory)
   bool packed = false;      // staged inputs: A, s, e go in one copy
+  // packed inputs in page-locked memory: that allocation's host range, so
+  // that inputs of requests admitted together that lie back to back in it
+  // (and in the pool) go in one copy; 0 otherwise
+  uintptr_t locked_lo = 0, locked_hi = 0;
   // device addresses of the caller's buffers (in place) or of the pool copies
   const int16_t *dA = nullptr, *ds = nullptr, *de = nullptr;
   int16_t* dout = nullptr;
@@ -113,6 +117,14 @@ struct tk_server {
   // (the fixed cost of each copy operation overlaps), and the pass's tail
   // write on h2d waits for all of them
   cudaStream_t h2d_more[kCopyStreams - 1] = {};
+  // the admission pass's pending input copy: packed inputs of consecutive
+  // requests, back to back in one page-locked allocation and in the pool
+  struct {
+    const uint8_t* src = nullptr;
+    uint8_t* dst = nullptr;
+    size_t bytes = 0;
+    uintptr_t lo = 0;
+  } run;
   cudaEvent_t copied[kCopyStreams - 1] = {};
   unsigned pass_streams = 0;  // bit i: h2d_more[i] took a copy in this pass
   unsigned next_stream = 0;
@@ -201,6 +213,43 @@ const void* mapped_host_range(const void* p, size_t bytes) {
   return a.devicePointer;
 }
 
+// The host range [lo, hi) of the page-locked allocation holding p, or false
+// (pageable memory, or no range query).
+bool locked_allocation(const void* p, uintptr_t* lo, uintptr_t* hi) {
+  static const auto get_attr = driver_fn<PFN_cuPointerGetAttribute_v4000>("cuPointerGetAttribute");
+  if (!p || !get_attr) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type != cudaMemoryTypeHost) return false;
+  CUdeviceptr start = 0;
+  size_t size = 0;
+  const CUdeviceptr dp = (CUdeviceptr)(a.devicePointer ? a.devicePointer : p);
+  if (get_attr(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, dp) != CUDA_SUCCESS ||
+      get_attr(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, dp) != CUDA_SUCCESS || dp < start)
+    return false;
+  *lo = (uintptr_t)p - (uintptr_t)(dp - start);  // the same offset in host addresses
+  *hi = *lo + size;
+  return true;
+}
+
+// Issues the pass's pending input copy on the next copy stream of the
+// rotation.
+cudaError_t flush_run(tk_server* S) {
+  if (!S->run.bytes) return cudaSuccess;
+  const unsigned k_st = S->next_stream++ % kCopyStreams;
+  cudaStream_t st = k_st == 0 ? S->h2d : S->h2d_more[k_st - 1];
+  if (k_st) S->pass_streams |= 1u << (k_st - 1);
+  const cudaError_t e =
+      cudaMemcpyAsync(S->run.dst, S->run.src, S->run.bytes, cudaMemcpyHostToDevice, st);
+  S->run.bytes = 0;
+  std::lock_guard<std::mutex> lk(S->mu);  // counters are read under the lock
+  S->counters.input_copies++;
+  return e;
+}
+
 // Staged inputs: copies into the request's pool block.  Every request: its
 // job descriptors into the ring.
 cudaError_t admit(tk_server* S, Request* r) {
@@ -215,17 +264,33 @@ cudaError_t admit(tk_server* S, Request* r) {
     int16_t* dA = (int16_t*)base;
     int16_t* ds = (int16_t*)(base + ab);
     int16_t* de = r->e ? (int16_t*)(base + ab + vb) : nullptr;
-    // this request's copies go to the next copy stream of the rotation
-    const unsigned k_st = S->next_stream++ % kCopyStreams;
-    cudaStream_t st = k_st == 0 ? S->h2d : S->h2d_more[k_st - 1];
-    if (k_st) S->pass_streams |= 1u << (k_st - 1);
-    cudaError_t e;
+    cudaError_t e = cudaSuccess;
     if (r->packed) {
-      e = cudaMemcpyAsync(dA, r->A, ab + vb * (r->e ? 2 : 1), cudaMemcpyHostToDevice, st);
+      // joins the pending copy when it continues it in host memory (the same
+      // page-locked allocation) and in the pool; else that copy goes out and
+      // this one becomes the pending one.  The pass's copies all go out before
+      // its tail is published.
+      const uint8_t* src = (const uint8_t*)r->A;
+      if (S->run.bytes && r->locked_lo && r->locked_lo == S->run.lo &&
+          S->run.src + S->run.bytes == src && S->run.dst + S->run.bytes == base) {
+        S->run.bytes += in_bytes;
+      } else {
+        e = flush_run(S);
+        S->run.src = src;
+        S->run.dst = base;
+        S->run.bytes = in_bytes;
+        S->run.lo = r->locked_lo;
+      }
     } else {
+      // this request's copies go to the next copy stream of the rotation
+      const unsigned k_st = S->next_stream++ % kCopyStreams;
+      cudaStream_t st = k_st == 0 ? S->h2d : S->h2d_more[k_st - 1];
+      if (k_st) S->pass_streams |= 1u << (k_st - 1);
       e = cudaMemcpyAsync(dA, r->A, ab, cudaMemcpyHostToDevice, st);
       if (e == cudaSuccess) e = cudaMemcpyAsync(ds, r->s, vb, cudaMemcpyHostToDevice, st);
       if (e == cudaSuccess && de) e = cudaMemcpyAsync(de, r->e, vb, cudaMemcpyHostToDevice, st);
+      std::lock_guard<std::mutex> lk(S->mu);  // counters are read under the lock
+      S->counters.input_copies += de ? 3 : 2;
     }
     if (e != cudaSuccess) return e;
     r->dA = dA;
@@ -280,6 +345,7 @@ cudaError_t ensure_kernel(tk_server* S) {
   if (e == cudaSuccess) e = cudaEventRecord(S->kernel_done, S->comp);
   if (e == cudaSuccess) {
     S->kernel_running = true;
+    std::lock_guard<std::mutex> lk(S->mu);  // counters are read under the lock
     S->counters.device_loop_launches++;
   }
   return e;
@@ -346,6 +412,7 @@ void scheduler(tk_server* S) {
       S->active.push_back(r);
       progress = true;
     }
+    if (err == cudaSuccess) err = flush_run(S);
     if (err == cudaSuccess && S->published != pub0) {
       err = publish(S);
       if (err == cudaSuccess) err = ensure_kernel(S);
@@ -555,6 +622,7 @@ int tk_server_submit(tk_server* S, int k, size_t njobs, const int16_t* A, const 
     }
     r->packed =
         !r->in_direct && back_to_back && tk::host_span_one_copy(A, ab + vb * (e ? 2 : 1));
+    if (r->packed && !locked_allocation(A, &r->locked_lo, &r->locked_hi)) r->locked_lo = 0;
     if (prev != S->device) cudaSetDevice(prev);
   }
   const size_t pool_bytes =

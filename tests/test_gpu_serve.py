@@ -179,3 +179,41 @@ def test_pinned_is_staged_without_zero_copy(tk, cuda, oracle):
         assert st["direct_outputs"] == 1
         assert st["queue_ns"] + st["device_ns"] + st["return_ns"] > 0
     assert (canon(out) == canon(oracle_out(oracle, k, A, s, e))).all()
+
+
+def test_back_to_back_requests_share_input_copies(tk, cuda, oracle):
+    """200 requests whose A | s | e lie back to back in one page-locked arena
+    (outputs page-locked too, written in place), submitted in one burst: once
+    64 are active, admission takes the next ones 32 at a time, and inputs that
+    continue each other in the arena and in the pool go in one copy.  Every
+    result equals the oracle's, and fewer input copies were issued than
+    requests staged."""
+    import torch
+    r = rng(4242)
+    reqs = [(int(r.integers(2, 5)), int(r.integers(16, 65))) for _ in range(200)]
+    sizes = [n * (k * k + 2 * k) * 256 for k, n in reqs]
+    arena = torch.empty(sum(sizes), dtype=torch.int16, pin_memory=True).numpy()
+    outs, views, off = [], [], 0
+    for i, ((k, n), sz) in enumerate(zip(reqs, sizes)):
+        A, s, e = request(5000 + i, k, n, uniform=True)
+        m = arena[off:off + sz]
+        pa = m[:A.size].reshape(A.shape)
+        ps = m[A.size:A.size + s.size].reshape(s.shape)
+        pe = m[A.size + s.size:].reshape(e.shape)
+        pa[...], ps[...], pe[...] = A, s, e
+        views.append((k, pa, ps, pe))
+        outs.append(pinned_copy(np.zeros_like(s)))
+        off += sz
+    with tk.Server(hbm_budget_bytes=1 << 30, max_inflight_requests=256) as srv:
+        st0 = srv.stats()
+        tickets = [srv.submit(k, A, s, e, out) for (k, A, s, e), out in zip(views, outs)]
+        for t in tickets:
+            srv.wait(t, timeout=60)
+            srv.release(t)
+        st = srv.stats()
+    staged = st["staged_requests"] - st0["staged_requests"]
+    copies = st["input_copies"] - st0["input_copies"]
+    assert staged == 200 and st["direct_outputs"] - st0["direct_outputs"] == 200
+    assert 0 < copies < staged, (copies, staged)
+    for (k, A, s, e), out in zip(views, outs):
+        assert (canon(out) == canon(oracle_out(oracle, k, A, s, e))).all()
