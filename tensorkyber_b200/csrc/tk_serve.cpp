@@ -4,7 +4,10 @@
 // memory.  Requests are admitted in arrival order.  A staged request needs a
 // block of the server's device pool (hbm_budget bytes) for its A, s, e and
 // out: admission copies the inputs in (one copy when the caller's A, s and e
-// are contiguous) and, after the jobs ran, the outputs are copied back.  When
+// are contiguous; one copy for several requests admitted in the same pass when
+// their inputs also lie back to back in one page-locked allocation and their
+// pool blocks are consecutive) and, after the jobs ran, the outputs are copied
+// back.  When
 // out is device-mapped page-locked host memory the device loop writes the
 // outputs there itself (posted PCIe writes; no pool block for out, no copy
 // back).  With zero_copy, inputs in such memory are read in place too (no
