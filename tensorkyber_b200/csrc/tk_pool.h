@@ -27,6 +27,35 @@ class Pool {
     }
     return false;
   }
+  // Next fit from `from` (the end of the previous allocation): [from, from +
+  // n) when it is free, else the first free range after from that fits, else
+  // the first fit from the start.  Requests that are admitted one after
+  // another and finish roughly in order so get consecutive ranges.
+  bool alloc_from(size_t n, size_t from, size_t* off) {
+    auto it = free_.upper_bound(from);
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);  // the free range starting at or before from
+      const size_t o = pv->first, len = pv->second;
+      if (from < o + len && o + len - from >= n) {
+        if (from > o)
+          pv->second = from - o;  // the part before from stays free
+        else
+          free_.erase(pv);
+        if (o + len > from + n) free_[from + n] = o + len - from - n;
+        *off = from;
+        return true;
+      }
+    }
+    for (; it != free_.end(); ++it) {
+      if (it->second < n) continue;
+      *off = it->first;
+      const size_t rest = it->second - n, o = it->first;
+      free_.erase(it);
+      if (rest) free_[o + n] = rest;
+      return true;
+    }
+    return alloc(n, off);
+  }
   void release(size_t off, size_t n) {
     auto it = free_.emplace(off, n).first;
     auto nx = std::next(it);

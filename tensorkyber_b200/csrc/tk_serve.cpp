@@ -4,29 +4,29 @@
 // memory.  Requests are admitted in arrival order.  A staged request needs a
 // block of the server's device pool (hbm_budget bytes) for its A, s, e and
 // out: admission copies the inputs in (one copy when the caller's A, s and e
-// are contiguous; one copy for several requests admitted in the same pass when
-// their inputs also lie back to back in one page-locked allocation and their
-// pool blocks are consecutive) and, after the jobs ran, the outputs are copied
-// back.  When
-// out is device-mapped page-locked host memory the device loop writes the
-// outputs there itself (posted PCIe writes; no pool block for out, no copy
-// back).  With zero_copy, inputs in such memory are read in place too (no
-// pool memory at all; uncached PCIe reads, slower than one bulk copy).  Admission writes one descriptor per job into the
-// job ring, which lives in mapped page-locked host memory (the device reads a
-// descriptor once, when it claims the job), and every admission pass then
-// publishes its jobs with one stream write of the new tail, behind the input
-// copies on the same stream.  A persistent kernel (k_serve, tk_matvec.cu)
-// claims published jobs as they appear: jobs of requests that arrive while
-// others are on the GPU join the running loop and run side by side with them.
-// When the last job of a request finishes, the kernel writes the request's
-// generation into a flag in mapped host memory; the scheduler thread then
-// completes the ticket (outputs in place) or copies the outputs back first (a
-// stream write after the copy raises a second flag).  Per request that is one
-// or three copy-engine operations in and one out, the cost that bounds the
-// request rate (each is a few microseconds however small).  The device loop exits on its own
-// after idle_exit seconds without work and is relaunched when work arrives.
-// No reference counterpart: the reference only times fixed batches
-// (ntt_bench.cu:600-903).
+// are contiguous; one copy for several requests admitted in the same pass
+// when their inputs also lie back to back in one page-locked allocation and
+// their pool blocks are consecutive, which next-fit allocation makes the
+// usual case) and, after the jobs ran, the outputs are copied back.  When out
+// is device-mapped page-locked host memory the device loop writes the outputs
+// there itself (posted PCIe writes; no pool block for out, no copy back).
+// With zero_copy, inputs in such memory are read in place too (no pool memory
+// at all; uncached PCIe reads, slower than one bulk copy).  Admission writes
+// one descriptor per job into the job ring, which lives in mapped page-locked
+// host memory (the device reads a descriptor once, when it claims the job),
+// and every admission pass then publishes its jobs with one stream write of
+// the new tail, behind the input copies on the same stream.  A persistent
+// kernel (k_serve, tk_matvec.cu) claims published jobs as they appear: jobs of
+// requests that arrive while others are on the GPU join the running loop and
+// run side by side with them.  When the last job of a request finishes, the
+// kernel writes the request's generation into a flag in mapped host memory;
+// the scheduler thread then completes the ticket (outputs in place) or copies
+// the outputs back first (a stream write after the copy raises a second
+// flag).  Per request that is up to three copy-engine operations in and one
+// out, the cost that bounds the request rate (each is a few microseconds
+// however small).  The device loop exits on its own after idle_exit seconds
+// without work and is relaunched when work arrives.  No reference
+// counterpart: the reference only times fixed batches (ntt_bench.cu:600-903).
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
@@ -84,10 +84,10 @@ struct Request {
   bool in_direct = false;   // inputs read in place (zero_copy)
   bool out_direct = false;  // outputs written in place (out is mapped pinned memory)
   bool packed = false;      // staged inputs: A, s, e go in one copy
-  // packed inputs in page-locked memory: that allocation's host range, so
-  // that inputs of requests admitted together that lie back to back in it
-  // (and in the pool) go in one copy; 0 otherwise
-  uintptr_t locked_lo = 0, locked_hi = 0;
+  // packed inputs in page-locked memory: the start of that allocation (host
+  // address), so that inputs of requests admitted together that lie back to
+  // back in it (and in the pool) go in one copy; 0 otherwise
+  uintptr_t locked_lo = 0;
   // device addresses of the caller's buffers (in place) or of the pool copies
   const int16_t *dA = nullptr, *ds = nullptr, *de = nullptr;
   int16_t* dout = nullptr;
@@ -108,6 +108,10 @@ struct tk_server {
   bool zero_copy = false;
   uint8_t* pool = nullptr;
   tk::Pool alloc;
+  // end of the last pool block handed out: the next request's block is taken
+  // from there (next fit), so consecutive requests get consecutive blocks and
+  // their inputs can share a copy
+  size_t alloc_end = 0;
   tk::ServeJob* ring = nullptr;       // job ring, mapped pinned host memory
   tk::ServeCtl* ctl = nullptr;
   unsigned int* req_ctr = nullptr;    // device
@@ -402,7 +406,8 @@ void scheduler(tk_server* S) {
         if (S->active.size() >= kMaxActive) break;  // backpressure on the copy queue
         Request* h = S->pending.front();
         if (S->published + h->njobs - oldest > kRingCap) break;
-        if (h->bytes && !S->alloc.alloc(h->bytes, &h->off)) break;
+        if (h->bytes && !S->alloc.alloc_from(h->bytes, S->alloc_end, &h->off)) break;
+        if (h->bytes) S->alloc_end = h->off + h->bytes;
         S->pending.pop_front();
         h->slot = S->free_slots.back();
         S->free_slots.pop_back();
@@ -625,7 +630,8 @@ int tk_server_submit(tk_server* S, int k, size_t njobs, const int16_t* A, const 
     }
     r->packed =
         !r->in_direct && back_to_back && tk::host_span_one_copy(A, ab + vb * (e ? 2 : 1));
-    if (r->packed && !locked_allocation(A, &r->locked_lo, &r->locked_hi)) r->locked_lo = 0;
+    uintptr_t locked_hi = 0;
+    if (r->packed && !locked_allocation(A, &r->locked_lo, &locked_hi)) r->locked_lo = 0;
     if (prev != S->device) cudaSetDevice(prev);
   }
   const size_t pool_bytes =

@@ -1,8 +1,12 @@
 """The server's device-pool allocator (tk_pool.h), driven on the CPU against
-a reference model: every range it hands out is the first free range that
-fits, lies inside the pool and overlaps nothing live; its free list stays
-sorted, disjoint and coalesced, and equals the complement of the live ranges;
-releasing everything restores one free range."""
+a reference model: every range it hands out is the one its policy names
+(first fit for alloc; for alloc_from, the hint itself when it starts room
+enough, else the first free range after it that fits, else the first fit),
+lies inside the pool and overlaps nothing live; its free list stays sorted,
+disjoint and coalesced, and equals the complement of the live ranges;
+releasing everything restores one free range.  With releases in allocation
+order (the server's requests finish roughly so), next fit hands out
+consecutive ranges."""
 import os
 import subprocess
 
@@ -11,6 +15,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DRIVER = r"""
 #include <stdio.h>
 #include <stdlib.h>
+#include <algorithm>
 #include <iterator>
 #include <map>
 #include <random>
@@ -22,34 +27,64 @@ static int fail(const char* what, long step) { printf("FAIL %s at %ld\n", what, 
 int main() {
   const size_t kSize = 1 << 20;
   std::mt19937_64 rng(20241204);
-  for (int round = 0; round < 4; round++) {
+  long adjacent = 0, fifo_allocs = 0;
+  for (int round = 0; round < 8; round++) {
+    const bool next_fit = round >= 4, fifo = round >= 6;
     tk::Pool P;
     P.init(kSize);
     std::map<size_t, size_t> live;  // offset -> length
+    std::vector<size_t> order;      // live offsets in allocation order (fifo rounds)
+    size_t hint = 0;                // end of the last allocation
     for (long step = 0; step < 50000; step++) {
-      const bool do_alloc = live.empty() || (rng() % 100) < (round == 3 ? 45u : 55u);
+      const bool do_alloc = live.empty() || (rng() % 100) < (round % 4 == 3 ? 45u : 55u);
       if (do_alloc) {
-        const size_t n = 1 + rng() % (round == 0 ? 64 : kSize / 16);
-        // expected: first gap (by offset) of length >= n in the complement of live
-        size_t want = (size_t)-1, cur = 0;
+        const size_t n = 1 + rng() % (round % 4 == 0 ? 64 : kSize / 16);
+        // the gaps (complement of live), by offset
+        std::vector<std::pair<size_t, size_t>> gaps;
+        size_t cur = 0;
         for (auto& r : live) {
-          if (r.first - cur >= n) { want = cur; break; }
+          if (r.first > cur) gaps.push_back({cur, r.first});
           cur = r.first + r.second;
         }
-        if (want == (size_t)-1 && kSize - cur >= n) want = cur;
+        if (cur < kSize) gaps.push_back({cur, kSize});
+        size_t want = (size_t)-1;
+        if (next_fit) {
+          for (auto& g : gaps)  // the hint inside a gap with room
+            if (g.first <= hint && hint < g.second && g.second - hint >= n) want = hint;
+          if (want == (size_t)-1)
+            for (auto& g : gaps)
+              if (g.first > hint && g.second - g.first >= n) { want = g.first; break; }
+        }
+        if (want == (size_t)-1)
+          for (auto& g : gaps)
+            if (g.second - g.first >= n) { want = g.first; break; }
         size_t off = 0;
-        const bool ok = P.alloc(n, &off);
+        const bool ok = next_fit ? P.alloc_from(n, hint, &off) : P.alloc(n, &off);
         if (ok != (want != (size_t)-1)) return fail("alloc success", step);
         if (ok) {
-          if (off != want) return fail("first fit", step);
+          if (off != want) return fail(next_fit ? "next fit" : "first fit", step);
           if (off + n > kSize) return fail("bounds", step);
+          if (fifo) {
+            fifo_allocs++;
+            adjacent += off == hint;
+          }
           live[off] = n;
+          order.push_back(off);
+          hint = off + n;
         }
       } else {
-        auto it = live.begin();
-        std::advance(it, rng() % live.size());
-        P.release(it->first, it->second);
-        live.erase(it);
+        // fifo rounds: mostly the oldest live range, as requests finish
+        size_t victim;
+        if (fifo && rng() % 8 != 0) {
+          victim = order.front();
+        } else {
+          auto it = live.begin();
+          std::advance(it, rng() % live.size());
+          victim = it->first;
+        }
+        order.erase(std::find(order.begin(), order.end(), victim));
+        P.release(victim, live[victim]);
+        live.erase(victim);
       }
       // the free list is the complement of live: sorted, disjoint, coalesced
       size_t cur = 0;
@@ -77,6 +112,11 @@ int main() {
     if (P.free_ranges().size() != 1 || P.free_ranges().begin()->first != 0 ||
         P.free_ranges().begin()->second != kSize)
       return fail("full recovery", -1);
+  }
+  // with releases in allocation order, next fit keeps most neighbours adjacent
+  if (adjacent * 10 < fifo_allocs * 6) {
+    printf("FAIL adjacency %ld of %ld\n", adjacent, fifo_allocs);
+    return 1;
   }
   printf("ok\n");
   return 0;
