@@ -36,6 +36,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -109,16 +110,60 @@ def config(npoly, world):
 
 # ------------------------------------------------------------------ clocks --
 class ClockSampler:
+    """SM clock, power and clock-event reasons of one GPU while it runs: NVML
+    polled every 2 ms from a thread (so that even a timed region of a few
+    milliseconds gets samples), or nvidia-smi at 100 ms where NVML cannot be
+    loaded.  The GPU is found by its PCI bus id, so the CUDA device number
+    need not be NVML's index.  Reads only; changes no setting."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
 
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self.stop_flag = threading.Event()
+
+            def one():
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx,
+                                  [n for n, bit in zip(self.REASONS, bits) if r & bit]))
+
+            def poll():
+                while not self.stop_flag.is_set():
+                    one()
+                    time.sleep(0.002)
+            self.sample_now = one
+            # the poller must get the interpreter while the caller launches
+            self.switch = sys.getswitchinterval()
+            sys.setswitchinterval(0.001)
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         fd, self.path = tempfile.mkstemp(prefix="tk_clocks_", suffix=".csv")
         os.close(fd)
         try:
@@ -131,6 +176,18 @@ class ClockSampler:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.sample_now()  # at least one sample at the end of the window
+            self.stop_flag.set()
+            self.thread.join(timeout=10)
+            sys.setswitchinterval(self.switch)
+            if not self.rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                        "source": "nvml"}
+            return {"sm_mhz": statistics.median(r[0] for r in self.rows),
+                    "sm_max_mhz": max(r[1] for r in self.rows),
+                    "reasons": sorted({n for r in self.rows for n in r[2]}),
+                    "samples": len(self.rows), "source": "nvml, every 2 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -146,11 +203,10 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        reasons = sorted({self.REASONS[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "source": "nvidia-smi, every 100 ms"}
 
 
 def load_peak():

@@ -58,3 +58,34 @@ def test_peak_and_traffic_sources():
         # algorithmic 1024 B per polynomial (L2 absorbs part of the writes)
         assert t is not None and 0 < t <= 1024 * 262144
     assert bench.load_traffic("no_such_kernel", 1) is None
+
+
+def test_clock_sampler_nvml_path(monkeypatch):
+    """The NVML path against a stand-in pynvml: clocks and event-reason bits
+    read every 2 ms while the sampler runs, so even a window of a few
+    milliseconds has samples; median and maximum clocks, reason names."""
+    import time
+    import types
+    fake = types.ModuleType("pynvml")
+    fake.NVML_CLOCK_SM = 1
+    fake.nvmlClocksEventReasonHwSlowdown = 0x8
+    fake.nvmlClocksEventReasonHwThermalSlowdown = 0x40
+    fake.nvmlClocksEventReasonSwThermalSlowdown = 0x20
+    fake.nvmlClocksEventReasonSwPowerCap = 0x4
+    clocks = iter([1965, 1800, 1900] * 1000)
+    fake.nvmlInit = lambda: None
+    fake.nvmlDeviceGetHandleByPciBusId = lambda bus: "h"
+    fake.nvmlDeviceGetHandleByIndex = lambda i: "h"
+    fake.nvmlDeviceGetMaxClockInfo = lambda h, c: 1965
+    fake.nvmlDeviceGetClockInfo = lambda h, c: next(clocks)
+    fake.nvmlDeviceGetCurrentClocksEventReasons = lambda h: 0x4 | 0x1   # power cap, idle
+    monkeypatch.setitem(sys.modules, "pynvml", fake)
+    sys.path.insert(0, ROOT)
+    import bench
+    s = bench.ClockSampler(0)
+    s.start()
+    time.sleep(0.02)
+    c = s.stop()
+    assert c["samples"] >= 3 and c["source"].startswith("nvml")
+    assert c["sm_mhz"] in (1800, 1900, 1965) and c["sm_max_mhz"] == 1965
+    assert c["reasons"] == ["sw_power_cap"]
