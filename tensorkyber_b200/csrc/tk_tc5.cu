@@ -47,7 +47,11 @@
 // group's chunk run while the other groups read theirs, and the next tile's
 // first stage starts while this tile's second-stage results are still being
 // read (an mbarrier, y_free, keeps the next tile's sums from being written
-// before both issuers' second-stage MMAs of this tile have read them).
+// before both issuers' second-stage MMAs of this tile have read them).  The
+// second stage's K step 0 reads only the sums of first-stage chunks 0-3,
+// which the epilogue warps write first: a second mbarrier, y_half, lets each
+// issuer start that step of its first two second-stage chunks while the other
+// half of the sums is still being written.
 // Three slots of 64 KiB: the load of tile k + 3 goes into tile k's slot once
 // tile k's output (written over its input) has been read out by the store.
 // Every mbarrier wait gives up after 2 s (status bit 0 forward / 1 inverse,
@@ -85,10 +89,11 @@ constexpr int kTcThreads = 32 * (kTcEpiWarps + kTcIssuers + 1);
 // dynamic shared memory (its base is 1024-byte aligned, the swizzle atom;
 // the kernel checks): three 64 KiB tile slots, this direction's constant
 // tiles, the mbarriers (in_full[3], out_ready[3], d_full[4], d_empty[4],
-// y_full, x_ready, x_read, consts, drain, y_free) and the tensor-memory base
+// y_full, x_ready, x_read, consts, drain, y_free, y_half) and the
+// tensor-memory base
 // address
 constexpr int kOffTables = kTcSlots * kTcSlotBytes;
-constexpr int kNumBars = 2 * kTcSlots + 2 * kTcGroups + 6;
+constexpr int kNumBars = 2 * kTcSlots + 2 * kTcGroups + 7;
 template <bool kInverse>
 struct Tc5Layout {
   static constexpr int kTiles = kInverse ? kTc5InvTiles : kTc5FwdTiles;
@@ -207,7 +212,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
   auto d_empty = [&](int g) { return bars + 8u * (2 * kTcSlots + kTcGroups + g); };
   constexpr uint32_t kB = 8u * (2 * kTcSlots + 2 * kTcGroups);
   const uint32_t y_full = bars + kB, x_ready = bars + kB + 8u, x_read = bars + kB + 16u,
-                 consts = bars + kB + 24u, drain = bars + kB + 32u, y_free = bars + kB + 40u;
+                 consts = bars + kB + 24u, drain = bars + kB + 32u, y_free = bars + kB + 40u,
+                 y_half = bars + kB + 48u;
   auto slot_addr = [&](int s) { return base + (uint32_t)s * kTcSlotBytes; };
 
   if (tid == 0) {
@@ -225,6 +231,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
     mbar_init(consts, 1);
     mbar_init(drain, kTcIssuers);
     mbar_init(y_free, kTcIssuers);
+    mbar_init(y_half, kTcEpiWarps);
     fence_mbar_init();
   }
   if (warp == kTcMmaWarp) {  // the first issuer's warp
@@ -338,24 +345,40 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
         }
         if (!ok) break;
         // second stage from tensor memory, two K steps per result: chunk b =
-        // g + 4 jj = results n = 4g + 2 jj, + 1
+        // g + 4 jj = results n = 4g + 2 jj, + 1.  K step h reads the sums of
+        // first-stage chunks 4h .. 4h + 3, so step 0 of the chunks jj = 0
+        // runs once that half is written (y_half), while the epilogue warps
+        // are still writing the other half; the rest waits for y_full.
+        auto b_mma = [&](int g, int jj, int h) {
+          const uint32_t dbuf = tmem + kColD0 + 64u * (uint32_t)g;
+#pragma unroll
+          for (int u = 0; u < 2; u++) {
+            const int n = 4 * g + 2 * jj + u;
+            tc_mma_ts(dbuf + 32u * u, tmem + kColY + 16u * (uint32_t)n + 8u * h,
+                      tile_desc(kInverse ? 32 + h : 36 + 2 * n + h), kIdescU8, h);
+          }
+        };
+        if (!(ok = mbar_wait_bounded(y_half, (uint32_t)k & 1u, kWaitNs))) break;
+        tc_fence_after();
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          if (!(ok = take(j + 2 * c, k, 2))) break;
+          b_mma(j + 2 * c, 0, 0);
+        }
+        if (!ok) break;
         if (!(ok = mbar_wait_bounded(y_full, (uint32_t)k & 1u, kWaitNs))) break;
         tc_fence_after();
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-          const int g = j + 2 * (c & 1), jj = c >> 1;
-          if (!(ok = take(g, k, 2 + jj))) break;
-          const uint32_t dbuf = tmem + kColD0 + 64u * (uint32_t)g;
-          const int n0 = 4 * g + 2 * jj;
+        for (int c = 0; c < 2; c++) {
+          b_mma(j + 2 * c, 0, 1);
+          tc_commit(d_full(j + 2 * c));
+        }
 #pragma unroll
-          for (int h = 0; h < 2; h++)
-#pragma unroll
-            for (int u = 0; u < 2; u++) {
-              const int n = n0 + u;
-              tc_mma_ts(dbuf + 32u * u, tmem + kColY + 16u * (uint32_t)n + 8u * h,
-                        tile_desc(kInverse ? 32 + h : 36 + 2 * n + h), kIdescU8, h);
-            }
-          tc_commit(d_full(g));
+        for (int c = 0; c < 2; c++) {
+          if (!(ok = take(j + 2 * c, k, 3))) break;
+          b_mma(j + 2 * c, 1, 0);
+          b_mma(j + 2 * c, 1, 1);
+          tc_commit(d_full(j + 2 * c));
         }
         if (!ok) break;
         // this issuer's reads of the first stage's sums are issued: the
@@ -445,6 +468,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc5(const __grid_constant__ T
         for (int n = 0; n < 16; n++)
           tc_st2(ycol + 16u * n + 2u * a, r[n] + (r[16 + n] << 7) + kFirstBias,
                  r[32 + n] + (r[48 + n] << 7) + kFirstBias);
+        if (jj == 0) {
+          // the sums of first-stage chunks 0-3 (columns 16 n .. 16 n + 7,
+          // the second stage's K step 0) are written once all 16 warps arrive
+          tc_wait_st();
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(y_half);
+        }
       }
       if (!ok) break;
       tc_wait_st();

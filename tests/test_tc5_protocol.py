@@ -13,8 +13,11 @@ is written only after its previous readers are done:
   * accumulator buffer g: MMAs only after the group released its previous
     contents; the group reads only completed results;
   * the first stage's sums in tensor memory: written for tile k only after
-    every second-stage MMA of tile k - 1 (both issuers) has completed; read
-    by the second stage only after all 16 warps wrote them.
+    every second-stage MMA of tile k - 1 (both issuers) has completed; each
+    second-stage K step (h = 0 reads the sums of first-stage chunks 0-3, h =
+    1 those of chunks 4-7) only after all 16 warps wrote its half: h = 0 of
+    a tile's first two second-stage chunks runs while the other half is
+    still being written.
 No GPU."""
 import random
 
@@ -55,6 +58,7 @@ class Sim:
         self.d_full = [Bar(1) for _ in range(GROUPS)]
         self.d_empty = [Bar(4) for _ in range(GROUPS)]
         self.y_full, self.x_ready, self.x_read = Bar(EPI_WARPS), Bar(EPI_WARPS), Bar(EPI_WARPS)
+        self.y_half = Bar(EPI_WARPS)
         self.y_free, self.drain = Bar(ISSUERS), Bar(ISSUERS)
         self.events = []                      # pending asynchronous completions
         self.mma_pending = [[] for _ in range(ISSUERS)]   # per issuer, in issue order
@@ -65,6 +69,7 @@ class Sim:
         self.buf_unread = [False] * GROUPS    # results written, not yet read out
         self.buf_writers = [0] * GROUPS       # MMAs in flight into the buffer
         self.y_writes = {}                    # tile -> warps that wrote its sums
+        self.y_half_writes = {}               # tile -> warps that wrote the first half
         self.y_readers = {}                   # tile -> its second-stage MMAs in flight
 
     # asynchronous work ------------------------------------------------------
@@ -72,13 +77,15 @@ class Sim:
         self.events.append(fn)
 
     def mma(self, issuer, kind, g, slot, tile):
-        """An MMA into buffer g; kind 'a' reads the slot, 'b' reads the sums
-        of `tile`."""
+        """An MMA into buffer g; kind 'a' reads the slot, 'b0' / 'b1' read the
+        first / second half of the sums of `tile` (second-stage K step h)."""
         assert not self.buf_unread[g], "MMA overwrites results the group has not read"
         self.buf_writers[g] += 1
         if kind == 'a':
             self.slot_readers[slot] += 1
         else:
+            written = self.y_half_writes if kind == 'b0' else self.y_writes
+            assert len(written.get(tile, ())) == EPI_WARPS, "second stage before its sums"
             self.y_readers[tile] = self.y_readers.get(tile, 0) + 1
         self.mma_pending[issuer].append((kind, g, slot, tile))
 
@@ -146,19 +153,39 @@ class Sim:
             else:
                 yield lambda: self.x_ready.ready(k & 1, k)
                 assert self.slot_tile[s] == ('transposed', k)
-            for stage in (0, 1):
-                if stage == 1:
-                    yield lambda: self.y_full.ready(k & 1, k)
-                    assert len(self.y_writes.get(k, ())) == EPI_WARPS
-                for c in range(4):
-                    g, jj = j + 2 * (c & 1), c >> 1
-                    pos = 2 * stage + jj
-                    if k > 0 or pos > 0:
-                        ph = 4 * k + pos - 1
-                        yield lambda g=g, ph=ph: self.d_empty[g].ready(ph & 1, ph)
-                    for _ in range(4):
-                        self.mma(j, 'a' if stage == 0 else 'b', g, s, k)
-                    self.commit(j, self.d_full[g], mark_buf=g)
+            def take(g, pos):
+                if k > 0 or pos > 0:
+                    ph = 4 * k + pos - 1
+                    return lambda: self.d_empty[g].ready(ph & 1, ph)
+                return lambda: True
+            for c in range(4):                    # first stage
+                g, jj = j + 2 * (c & 1), c >> 1
+                yield take(g, jj)
+                for _ in range(4):
+                    self.mma(j, 'a', g, s, k)
+                self.commit(j, self.d_full[g], mark_buf=g)
+            # second stage: K step 0 of chunks c = 0, 1 once the first half
+            # of the sums is written, the rest once all of them are
+            yield lambda: self.y_half.ready(k & 1, k)
+            for c in range(2):
+                g = j + 2 * c
+                yield take(g, 2)
+                for _ in range(2):
+                    self.mma(j, 'b0', g, s, k)
+            yield lambda: self.y_full.ready(k & 1, k)
+            for c in range(2):
+                g = j + 2 * c
+                for _ in range(2):
+                    self.mma(j, 'b1', g, s, k)
+                self.commit(j, self.d_full[g], mark_buf=g)
+            for c in range(2):
+                g = j + 2 * c
+                yield take(g, 3)
+                for _ in range(2):
+                    self.mma(j, 'b0', g, s, k)
+                for _ in range(2):
+                    self.mma(j, 'b1', g, s, k)
+                self.commit(j, self.d_full[g], mark_buf=g)
             self.commit(j, self.y_free)
         self.commit(j, self.drain)
         yield lambda: self.drain.ready(0, 0)
@@ -211,6 +238,9 @@ class Sim:
                     yield lambda: self.y_free.ready((k - 1) & 1, k - 1)
                 # sums of tile k over those of tile k - 1: its second stage is done
                 assert self.y_readers.get(k - 1, 0) == 0, "sums overwritten in use"
+                if jj == 0:                      # the first half of the sums written
+                    self.y_half_writes.setdefault(k, set()).add(w)
+                    self.y_half.arrive()
             self.y_writes.setdefault(k, set()).add(w)
             self.y_full.arrive()
             if not self.inv and k + 1 < self.n:
