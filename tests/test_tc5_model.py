@@ -252,3 +252,22 @@ def test_forward_output_addresses_are_the_tma_swizzle_layout():
                     assert a + 2 * u == (e // 64) * 16384 + p * 128 + (((w // 16) ^ (p % 8)) << 4) + w % 16
                 seen[a:a + 16] += 1
     assert (seen == 1).all()
+
+
+def test_first_half_of_the_sums_is_the_second_stage_step_zero():
+    """The epilogue group g writes first-stage chunk a = g + 4 jj (results
+    2a, 2a + 1) into tensor-memory columns 16 n + 2a + u of every output n;
+    the second stage's K step h of output n reads the eight columns 16 n + 8 h
+    .. + 7.  So the four groups' chunks jj = 0 (the y_half barrier) fill
+    exactly the columns of step 0 for every n, and those of jj = 1 exactly
+    step 1: step 0 may start after the first half, and the halves never
+    share a column."""
+    for n in range(16):
+        written = {0: set(), 1: set()}
+        for g in range(4):
+            for jj in range(2):
+                a = g + 4 * jj
+                for u in range(2):
+                    written[jj].add(16 * n + 2 * a + u)
+        for h in range(2):
+            assert written[h] == set(range(16 * n + 8 * h, 16 * n + 8 * h + 8))
