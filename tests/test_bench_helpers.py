@@ -1,6 +1,6 @@
 """bench.py's host helpers on the CPU: the clock sampler against a stand-in
 nvidia-smi that prints fixed rows (median and maximum clocks, the throttle
-reasons a run is judged by), and the roofline's peak and traffic sources."""
+reasons that reject a run), and the roofline's peak and traffic sources."""
 import os
 import sys
 
