@@ -174,10 +174,10 @@ __device__ __forceinline__ uint32_t sw128_chunk(uint32_t slot, uint32_t p, uint3
 // n + 1: inverse coefficients, forward blocks); chunk a or b goes to buffer
 // (and warp group) a % 4 or b % 4, issued by issuer (a or b) % 2, so group g
 // reads first-stage chunks g, g+4 and the second-stage results 4g .. 4g + 3.
-// The MMAs of one chunk can run
-// while the other groups read theirs; the second stage waits for the whole
-// first stage in tensor memory (y_full), the next tile's first stage only
-// for its buffers.
+// The MMAs of one chunk can run while the other groups read theirs.  The
+// second stage's K step 0 waits for the first half of the sums in tensor
+// memory (first-stage chunks 0-3, y_half), its K step 1 for all of them
+// (y_full); the next tile's first stage waits only for its buffers.
 //
 // The forward's transposition: for coefficient c (c-tile c, 4 KiB at 4096 c
 // of the slot), row p's 32 K bytes are the blocks' values X[m][c] in block
